@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of the spherical-harmonic transform hot path on B200.
+
+Workload (one "step"): one synthesis + one analysis ("an SHT pair", the
+reference's round trip, scripts/bench-sht.ts:7-9) of B = 256 real fields at
+lmax = mmax = 255 on the 384 x 768 Gauss grid, coefficients seeded Gaussian
+scaled by (l+1)^-1.  Spectral buffers ping-pong as in bench-sht.ts:160-205.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  ``value`` = SHT pairs/s over all ranks (inputs
+resident in HBM); ``e2e`` = the same with the step's coefficients copied
+host->device and the result device->host (pinned) inside the timed region.
+``--impl reference`` times the CPU restatement of the reference's f64
+transform (the reference itself is TypeScript/WebGPU and cannot run here) on
+the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LMAX = 255
+BATCH = 256
+METRIC = "IMEX steps/s & SHT pairs/s @lmax255: TC+batched vs plain FP32, <=1e-5 vs f64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--lmax", type=int, default=LMAX)
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--precision", default="fp32")
+    return ap.parse_args()
+
+
+def grid(lmax):
+    nlat = (3 * (lmax + 1) + 1) // 2
+    nlat += nlat & 1
+    return nlat, 2 * nlat
+
+
+def spectrum(lmax, seed):
+    """Seeded Gaussian coefficients scaled by (l+1)^-1, m = 0 imaginary zero."""
+    rng = np.random.default_rng(seed)
+    q = rng.standard_normal((lmax + 1) * (lmax + 2)).astype(np.float32)
+    l_of = np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
+    m_of = np.concatenate([np.full(lmax + 1 - m, m) for m in range(lmax + 1)])
+    q = q.reshape(-1, 2) / (l_of[:, None] + 1.0)
+    q[m_of == 0, 1] = 0.0
+    return np.ascontiguousarray(q.ravel(), dtype=np.float32)
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+        0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+        0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+    }
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.ok = [], 0, False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+        self._stop = threading.Event()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                self.reasons |= self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            except Exception:
+                pass
+            time.sleep(0.05)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["nvml unavailable"]}
+        names = [n for b, n in self.REASONS.items() if self.reasons & b and n != "gpu_idle"]
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": names, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            p = json.load(fh)
+        return p.get("hbm_gbs", 6650.0), p.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def cpu_baseline(lmax, nlat, nphi, budget_s=10.0, threads=0):
+    """The f64 oracle transform on the host cores: SHT pairs/s on a bounded
+    sample of the same workload (as many single-field pairs as fit the budget)."""
+    from oracle import oracle as O
+    ref = O.ShtReference(lmax, lmax, nlat, nphi, threads=threads)
+    q = spectrum(lmax, 0).astype(np.float64)
+    t0 = time.perf_counter()
+    ref.analys(ref.synth(q))
+    one = time.perf_counter() - t0
+    n = max(1, min(200, int(budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    for i in range(n):
+        q = ref.analys(ref.synth(q))
+    dt = time.perf_counter() - t0
+    cores = threads or os.cpu_count()
+    return {"value": n / dt, "unit": "SHT pairs/s", "cores": cores, "kind": "port",
+            "sample": f"{n} single-field pairs at lmax {lmax} ({nlat}x{nphi}), f64 direct "
+                      f"summation (oracle restating src/sht/reference.ts), {dt:.1f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU transform path, restated (oracle)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    lmax = args.lmax
+    nlat, nphi = grid(lmax)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi, threads=0)
+    q = spectrum(lmax, 0).astype(np.float64)
+    per_step = 2  # single-field pairs per step: a bounded sample of the batch
+    for _ in range(args.warmup):
+        q = ref.analys(ref.synth(q))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for _ in range(per_step):
+            q = ref.analys(ref.synth(q))
+    dt = time.perf_counter() - t0
+    value = per_step * args.steps / dt
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "SHT pairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"SHT round trip, lmax {lmax}, {nlat}x{nphi} Gauss grid, "
+                               f"{per_step} fields/step sample of the B={args.batch} batch"},
+        "cpu_baseline": {"value": value, "unit": "SHT pairs/s", "cores": cores, "kind": "port",
+                         "sample": f"{per_step} single-field pairs per step, f64 oracle "
+                                   "(src/sht/reference.ts restated in C, OpenMP)"},
+        "e2e": {"value": value, "unit": "SHT pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from turing_sphere_b200 import ShtConfig, ShtPlan, Device
+    from turing_sphere_b200.sht import bytes_per_pair, flop_per_pair
+
+    lmax, B = args.lmax, args.batch
+    nlat, nphi = grid(lmax)
+    dev = Device(local)
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    plan = ShtPlan.create(dev, ShtConfig(lmax, lmax, nlat, nphi), {"precision": args.precision})
+    nlm = plan.nlm
+
+    q0 = np.stack([spectrum(lmax, 1000 * rank + b) for b in range(B)])
+    qa = torch.from_numpy(q0).cuda()
+    qb = torch.empty_like(qa)
+    spat = torch.empty(B, nlat * nphi, device="cuda")
+    fm = torch.empty(B, 2 * (lmax + 1) * nlat, device="cuda")
+    sp = stream.cuda_stream
+
+    # correctness guard before timing (bench-sht.ts:252-318): one round trip
+    plan.synth_dev(qa.data_ptr(), spat.data_ptr(), B, sp)
+    plan.analys_dev(spat.data_ptr(), qb.data_ptr(), B, sp)
+    torch.cuda.synchronize()
+    rt = float(torch.linalg.vector_norm(qb - qa) / torch.linalg.vector_norm(qa))
+    if not math.isfinite(rt) or rt > 1e-3:
+        print(json.dumps({"error": f"round trip relL2 {rt}"}), flush=True)
+        return 1
+
+    bufs = [qa, qb]
+    stages = ["legSynth", "fourSynth", "fourAnalys", "legAnalys"]
+
+    def step(i, ev=None):
+        src, dst = bufs[i & 1], bufs[(i + 1) & 1]
+        ins = [src, fm, spat, fm]
+        outs = [fm, spat, fm, dst]
+        for k, st in enumerate(stages):
+            if ev is not None:
+                ev[k].record(stream)
+            plan.stage_dev(st, ins[k].data_ptr(), outs[k].data_ptr(), B, sp)
+        if ev is not None:
+            ev[4].record(stream)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+
+    K = args.steps
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(K)]
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with sampler:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(K):
+            step(i, evs[i])
+        t1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    stage_ms = np.zeros(4)
+    for e in evs:
+        for k in range(4):
+            stage_ms[k] += e[k].elapsed_time(e[k + 1])
+    stage_ms /= K
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # end to end: pinned host coefficients in, result out, every step
+    hq_in = torch.from_numpy(q0).pin_memory()
+    hq_out = torch.empty_like(hq_in).pin_memory()
+    Ke = max(3, K // 4)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(Ke):
+        qa.copy_(hq_in, non_blocking=True)
+        plan.synth_dev(qa.data_ptr(), spat.data_ptr(), B, sp)
+        plan.analys_dev(spat.data_ptr(), qb.data_ptr(), B, sp)
+        hq_out.copy_(qb, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    back = hq_out.numpy()
+    e2e_err = float(np.sqrt(((back - q0) ** 2).sum() / (q0 ** 2).sum()))
+
+    if rank == 0:
+        hbm, bf16, src = measured_peaks()
+        pairs = world * B * K
+        value = pairs / (ms / 1e3)
+        # dominant kernel: the slowest stage
+        k = int(np.argmax(stage_ms))
+        name = stages[k]
+        nlm_b = 8.0 * nlm * B
+        fm_b = 8.0 * (lmax + 1) * nlat * B
+        sp_b = 4.0 * nlat * nphi * B
+        alg_bytes = [nlm_b + fm_b, fm_b + sp_b, sp_b + fm_b, fm_b + nlm_b][k]
+        leg_flop = 2.0 * nlm * nlat * B
+        fft_flop = 2.5 * nphi * math.log2(nphi) * nlat * B
+        alg_flop = [leg_flop, fft_flop, fft_flop, leg_flop][k]
+        dur = stage_ms[k] / 1e3
+        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 SIMT TFLOP/s
+        if name.startswith("leg"):
+            roof = {"kernel": name, "bound": "fp32", "achieved": alg_flop / dur / 1e12,
+                    "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": alg_flop / dur / 1e12 / fp32_peak, "traffic": None,
+                    "peak_source": "nominal FP32 SIMT (148 SMs x 128 lanes x 2 x 1965 MHz); "
+                                   "no measured FP32 peak exists",
+                    "hbm_achieved_gbs": alg_bytes / dur / 1e9}
+        else:
+            roof = {"kernel": name, "bound": "hbm", "achieved": alg_bytes / dur / 1e9,
+                    "peak": hbm, "unit": "GB/s", "frac": alg_bytes / dur / 1e9 / hbm,
+                    "traffic": None, "peak_source": f"{src} hbm_gbs"}
+        roof["stage_ms"] = {s: float(v) for s, v in zip(stages, stage_ms)}
+        cpu = cpu_baseline(lmax, nlat, nphi, budget_s=10.0, threads=0)
+        line = {
+            "metric": METRIC, "value": value, "unit": "SHT pairs/s", "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": ms / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched SHT round trip (synth+analys), lmax=mmax={lmax}, "
+                                   f"{nlat}x{nphi} Gauss grid, B={B} fields per GPU",
+                       "precision": args.precision, "fourier": plan.fourierMode,
+                       "fft_radices": plan.fftRadices, "global_batch": B * world,
+                       "l2": f"inputs larger than L2 (grid fields {sp_b / 1e6:.0f} MB/step)"},
+            "e2e": {"value": world * B * Ke / (ems / 1e3), "unit": "SHT pairs/s",
+                    "h2d_bytes_per_step": int(nlm_b), "d2h_bytes_per_step": int(nlm_b),
+                    "round_trip_rel_l2": e2e_err},
+            "gpu_launches": 4 * K,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": sampler.summary(),
+            "round_trip_rel_l2": rt,
+            "flop_per_pair": flop_per_pair(lmax, lmax, nlat, nphi),
+            "bytes_per_pair": bytes_per_pair(lmax, lmax, nlat, nphi),
+        }
+        print(json.dumps(line), flush=True)
+    plan.destroy()
+    dev.destroy()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,137 @@
+/*
+ * turing_sht.h — C ABI of libturing_sht.so, the B200 (sm_100a) implementation
+ * of turing-sphere's spherical-harmonic transforms and IMEX model step.
+ *
+ * This is the drop-in boundary for the reference's WebGPU path: a host
+ * binding (the TypeScript side through N-API/koffi, or Python through ctypes)
+ * calls these functions where the reference installs a WebGPU device
+ * (scripts/nodeWebGpu.ts:18-65) and drives ShtPlan (src/sht/sht.ts),
+ * ModelPlan (src/mgpu/plan.ts) and GpuModel (src/mgpu/model.ts).
+ *
+ * Rules of the ABI:
+ *   - plain C types only: pointers, sizes, ints, floats; opaque handles;
+ *   - every function returns a status (TS_OK = 0, negative = error) and never
+ *     throws; ts_last_error(ctx) returns the message of the last failure on
+ *     that context;
+ *   - `_dev` entry points take device pointers and a cudaStream_t passed as
+ *     void* (NULL = the context's stream) and return without synchronising;
+ *     the others take caller-owned HOST arrays and block until done;
+ *   - one host thread per context.
+ *
+ * Layouts (src/sht/layout.ts:1-16): spectral arrays are float pairs
+ * [re, im] per coefficient in m-major order lm(l,m) = m(lmax+1) - m(m-1)/2 +
+ * (l-m), length 2*nlm per field; spatial arrays are float[nlat*nphi] per
+ * field, spat[ilat*nphi + iphi], ilat north to south.  A batch of B fields is
+ * B such arrays back to back.
+ */
+#ifndef TURING_SHT_H
+#define TURING_SHT_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ts_ctx_s *ts_ctx;
+typedef struct ts_plan_s *ts_plan;
+typedef struct ts_model_s *ts_model;
+
+enum ts_status {
+  TS_OK = 0,
+  TS_ERR_INVALID = -1,     /* bad argument or configuration */
+  TS_ERR_CUDA = -2,        /* a CUDA runtime/driver call failed */
+  TS_ERR_COMPILE = -3,     /* model source rejected (see ts_model_compile) */
+  TS_ERR_NOT_FOUND = -4,   /* unknown name */
+  TS_ERR_SIZE = -5,        /* length mismatch */
+  TS_ERR_UNSUPPORTED = -6, /* valid request this build does not implement */
+  TS_ERR_TIMEOUT = -7,     /* a bounded device-side wait gave up */
+  TS_ERR_STATE = -8        /* call out of order (e.g. read before run) */
+};
+
+/* Plan flags (bitwise OR). */
+enum ts_plan_flags {
+  TS_PREC_FP32 = 0,        /* plain FP32 on-the-fly recurrence (default) */
+  TS_PREC_TF32X3 = 1,      /* tcgen05 tensor-core Legendre, 3-pass split TF32 */
+  TS_PREC_BF16X3 = 2,      /* tcgen05 tensor-core Legendre, 3-pass split BF16 */
+  TS_PREC_MASK = 0xF,
+  TS_FOURIER_AUTO = 0,     /* mixed-radix FFT whenever nphi = 2^a 3^b, else DFT */
+  TS_FOURIER_FFT = 0x10,   /* require the FFT (error if nphi has other factors) */
+  TS_FOURIER_DFT = 0x20,   /* direct band-limited sum (sht.ts:241-289 semantics) */
+  TS_FOURIER_MASK = 0x30
+};
+
+/* ------------------------------------------------------------ context
+ * Replaces installWebGpu()/requestShtDevice() (scripts/nodeWebGpu.ts:18-65,
+ * src/sht/sht.ts:495-513): one CUDA device and one stream. */
+int ts_ctx_create(int device_ordinal, ts_ctx *out);
+int ts_ctx_destroy(ts_ctx ctx);
+const char *ts_last_error(ts_ctx ctx);
+/* Use an external cudaStream_t (as void*) for this context's work; NULL
+ * restores the context's own stream. */
+int ts_ctx_set_stream(ts_ctx ctx, void *stream);
+void *ts_ctx_stream(ts_ctx ctx);
+/* GPU name into buf (describeAdapter, sht.ts:464-493). */
+int ts_ctx_device_name(ts_ctx ctx, char *buf, size_t cap);
+/* Wait for all work on the context's stream (GPUQueue.onSubmittedWorkDone,
+ * session.ts:167-169). */
+int ts_sync(ts_ctx ctx);
+
+/* ------------------------------------------------------------- layout
+ * src/sht/layout.ts:24-59. */
+long ts_nlm_calc(int lmax, int mmax);
+long ts_lm_index(int lmax, int l, int m);
+/* 0 if valid, else TS_ERR_INVALID with the reason in buf (validateConfig). */
+int ts_validate_config(int lmax, int mmax, int nlat, int nphi, char *buf, size_t cap);
+void ts_grid_for_lmax(int lmax, int pdeg, int *nlat, int *nphi);
+
+/* ------------------------------------------------------------ SHT plan
+ * ShtPlan.create (sht.ts:166-183): validates the config, computes the
+ * Gauss-Legendre nodes/weights and the recurrence coefficients in FP64 on the
+ * GPU, and uploads FP32 tables.  flags: ts_plan_flags. */
+int ts_sht_plan_create(ts_ctx ctx, int lmax, int mmax, int nlat, int nphi, int flags,
+                       ts_plan *out);
+int ts_sht_plan_destroy(ts_plan plan);
+
+typedef struct ts_plan_info {
+  int lmax, mmax, nlat, nphi;
+  long nlm;
+  int precision;  /* TS_PREC_* in use */
+  int fourier;    /* TS_FOURIER_FFT or TS_FOURIER_DFT in use */
+  int fft_stages; /* Stockham stages of the nphi/2-point FFT (0 for DFT) */
+  int fft_radix[16];
+} ts_plan_info;
+int ts_sht_plan_info(ts_plan plan, ts_plan_info *info);
+
+/* Nodes x_i = cos(theta_i) (decreasing) and Gauss weights w_i, f64, nlat each,
+ * as computed on the GPU (ShtPlan.cosTheta / gaussWeights, sht.ts:120-125). */
+int ts_sht_plan_nodes(ts_plan plan, double *cos_theta, double *weights);
+
+/* Batched transforms on device pointers.  synth: qlm[B][2*nlm] ->
+ * spat[B][nlat*nphi]; analys: the reverse.  The fm intermediate is plan-owned
+ * scratch, grown on first use for a larger batch (encodeSynthInto /
+ * encodeAnalysInto, sht.ts:326-353; the scratch is sht.ts:291-298's fmBuf). */
+int ts_sht_synth_dev(ts_plan plan, const float *qlm, float *spat, int batch, void *stream);
+int ts_sht_analys_dev(ts_plan plan, const float *spat, float *qlm, int batch, void *stream);
+
+/* Blocking transforms on host arrays (ShtPlan.synth / ShtPlan.analys,
+ * sht.ts:414-461); they fail with TS_ERR_SIZE on a length mismatch. */
+int ts_sht_synth(ts_plan plan, const float *qlm, long qlm_len, float *spat, long spat_len,
+                 int batch);
+int ts_sht_analys(ts_plan plan, const float *spat, long spat_len, float *qlm, long qlm_len,
+                  int batch);
+
+/* Single stages, for diagnostics (ShtPlan.encodeStage, sht.ts:362-401;
+ * scripts/diagnose-sht.ts).  fm is [B][mmax+1][nlat] complex (2 floats). */
+int ts_sht_leg_synth_dev(ts_plan plan, const float *qlm, float *fm, int batch, void *stream);
+int ts_sht_fourier_synth_dev(ts_plan plan, const float *fm, float *spat, int batch,
+                             void *stream);
+int ts_sht_fourier_analys_dev(ts_plan plan, const float *spat, float *fm, int batch,
+                              void *stream);
+int ts_sht_leg_analys_dev(ts_plan plan, const float *fm, float *qlm, int batch, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TURING_SHT_H */

@@ -1,0 +1,192 @@
+"""Parity of the CUDA transforms with the f64 oracle, through the C ABI.
+
+Tolerance: relative L2 per transform <= 1e-5 against the f64 oracle on the
+same fp32 inputs (the target of the configurations), and the reference's own
+transformChecks bound of 1e-4 (test/transformChecks.ts:25-55) on its case.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from turing_sphere_b200 import ShtConfig, ShtPlan, gaussGrid, gridForLmax
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def make(device, lmax, nlat, nphi, mmax=None, **opts):
+    mmax = lmax if mmax is None else mmax
+    return ShtPlan.create(device, ShtConfig(lmax, mmax, nlat, nphi), opts)
+
+
+def scaled_spectrum(lmax, mmax, seed):
+    """Seeded Gaussian coefficients scaled by (l+1)^-1, m = 0 imaginary zero."""
+    rng = np.random.default_rng(seed)
+    nlm = O.nlm_calc(lmax, mmax)
+    q = rng.standard_normal(2 * nlm).astype(np.float64)
+    for m in range(mmax + 1):
+        for l in range(m, lmax + 1):
+            i = O.lm_index(lmax, l, m)
+            q[2 * i] /= (l + 1)
+            q[2 * i + 1] = 0.0 if m == 0 else q[2 * i + 1] / (l + 1)
+    return q.astype(np.float32)
+
+
+def test_transform_checks_reference_case(device):
+    """transformChecks.ts:25-55: lmax 31, gridForLmax(31, 1), randomSpectrum seed 42."""
+    lmax = 31
+    nlat, nphi = gridForLmax(lmax, 1)
+    plan = make(device, lmax, nlat, nphi)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = O.random_spectrum(lmax, lmax, 42)
+    spat_gpu = plan.synth(q)
+    spat_cpu = ref.synth(q.astype(np.float64))
+    e_s = O.rel_l2(spat_gpu, spat_cpu)
+    q_gpu = plan.analys(spat_cpu.astype(np.float32))
+    q_cpu = ref.analys(spat_cpu)
+    e_a = O.rel_l2(q_gpu, q_cpu)
+    assert e_s < 1e-4 and e_a < 1e-4
+    assert e_s < TOL and e_a < TOL, (e_s, e_a)
+
+
+GRIDS = [
+    (63, 96, 192), (127, 192, 384), (255, 384, 768),      # 3(l+1)/2 Gauss grids, nphi = 3*2^k
+    (63, 128, 256), (31, 48, 96), (15, 16, 32), (40, 64, 96),
+]
+
+
+@pytest.mark.parametrize("lmax,nlat,nphi", GRIDS)
+def test_synth_analys_parity(device, lmax, nlat, nphi):
+    plan = make(device, lmax, nlat, nphi)
+    assert plan.fourierMode == "fft"
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = scaled_spectrum(lmax, lmax, 7)
+    s_cpu = ref.synth(q.astype(np.float64))
+    e_s = O.rel_l2(plan.synth(q), s_cpu)
+    s32 = s_cpu.astype(np.float32)
+    e_a = O.rel_l2(plan.analys(s32), ref.analys(s32.astype(np.float64)))
+    assert e_s < TOL and e_a < TOL, (e_s, e_a)
+
+
+def test_nodes_and_weights_fp64_on_gpu(device):
+    for lmax, nlat, nphi in [(255, 384, 768), (31, 33, 64)]:
+        plan = make(device, lmax, nlat, nphi)
+        x, w = O.gauss(nlat)
+        assert np.abs(plan.cosTheta - x).max() < 2e-15
+        assert np.abs(plan.gaussWeights - w).max() < 1e-14
+
+
+def test_batched_equals_single(device):
+    lmax, (nlat, nphi) = 63, gaussGrid(63)
+    plan = make(device, lmax, nlat, nphi)
+    B = 11
+    qs = np.stack([scaled_spectrum(lmax, lmax, 100 + b) for b in range(B)])
+    sb = plan.synth(qs, batch=B).reshape(B, -1)
+    for b in (0, 5, 10):
+        assert O.rel_l2(sb[b], plan.synth(qs[b])) < 1e-6
+    qb = plan.analys(sb, batch=B).reshape(B, -1)
+    for b in (0, 4, 10):
+        assert O.rel_l2(qb[b], plan.analys(sb[b])) < 1e-6
+        assert O.rel_l2(qb[b], qs[b]) < 1e-5
+
+
+def test_round_trip_guard_lmax255(device):
+    """bench-sht.ts:252-318: one round trip returns the input (< 1e-3)."""
+    lmax, (nlat, nphi) = 255, gaussGrid(255)
+    plan = make(device, lmax, nlat, nphi)
+    q = O.seeded_spectrum(lmax, lmax, 1)
+    back = plan.analys(plan.synth(q))
+    assert np.isfinite(back).all()
+    assert O.rel_l2(back, q) < 1e-5
+
+
+@pytest.mark.parametrize("lmax,nlat,nphi,mmax", [
+    (31, 33, 64, 31),    # odd nlat: equator node, no pair
+    (31, 32, 100, 31),   # nphi = 4 * 25: DFT stage
+    (40, 48, 96, 20),    # mmax < lmax
+    (1, 2, 4, 1),        # smallest grid
+])
+def test_edge_grids(device, lmax, nlat, nphi, mmax):
+    plan = make(device, lmax, nlat, nphi, mmax=mmax)
+    ref = O.ShtReference(lmax, mmax, nlat, nphi)
+    q = scaled_spectrum(lmax, mmax, 3)
+    s_cpu = ref.synth(q.astype(np.float64))
+    assert O.rel_l2(plan.synth(q), s_cpu) < TOL
+    s32 = s_cpu.astype(np.float32)
+    assert O.rel_l2(plan.analys(s32), ref.analys(s32.astype(np.float64))) < TOL
+
+
+def test_forced_dft_matches_fft(device):
+    lmax, nlat, nphi = 63, 96, 192
+    a = make(device, lmax, nlat, nphi)
+    b = make(device, lmax, nlat, nphi, fourier="dft")
+    assert a.fourierMode == "fft" and b.fourierMode == "dft"
+    q = scaled_spectrum(lmax, lmax, 5)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    s_cpu = ref.synth(q.astype(np.float64))
+    assert O.rel_l2(b.synth(q), s_cpu) < TOL
+    assert O.rel_l2(b.analys(s_cpu.astype(np.float32)), ref.analys(s_cpu)) < TOL
+
+
+def test_stage_diagnostics(device):
+    """Per-stage parity (scripts/diagnose-sht.ts: Legendre vs Fourier stage)."""
+    import torch
+    lmax, nlat, nphi = 127, 192, 384
+    plan = make(device, lmax, nlat, nphi)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = scaled_spectrum(lmax, lmax, 11)
+    fm_ref = ref.legendre_synth(q.astype(np.float64))
+    qd = torch.from_numpy(q).cuda()
+    fm = torch.empty(2 * (lmax + 1) * nlat, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    plan.stage_dev("legSynth", qd.data_ptr(), fm.data_ptr(), 1, stream)
+    torch.cuda.synchronize()
+    assert O.rel_l2(fm.cpu().numpy(), fm_ref) < TOL
+    spat = torch.empty(nlat * nphi, dtype=torch.float32, device="cuda")
+    fm_in = torch.from_numpy(fm_ref.astype(np.float32)).cuda()
+    plan.stage_dev("fourSynth", fm_in.data_ptr(), spat.data_ptr(), 1, stream)
+    torch.cuda.synchronize()
+    assert O.rel_l2(spat.cpu().numpy(), ref.fourier_synth(fm_ref)) < TOL
+    s_ref = ref.synth(q.astype(np.float64)).astype(np.float32)
+    s_in = torch.from_numpy(s_ref).cuda()
+    plan.stage_dev("fourAnalys", s_in.data_ptr(), fm.data_ptr(), 1, stream)
+    torch.cuda.synchronize()
+    g_ref = ref.fourier_analys(s_ref.astype(np.float64))
+    # the GPU stage is unnormalised (2 pi / nphi lives in the Gauss weights)
+    assert O.rel_l2(fm.cpu().numpy() * (2 * np.pi / nphi), g_ref) < TOL
+    qo = torch.empty_like(qd)
+    gd = torch.from_numpy((g_ref / (2 * np.pi / nphi)).astype(np.float32)).cuda()
+    plan.stage_dev("legAnalys", gd.data_ptr(), qo.data_ptr(), 1, stream)
+    torch.cuda.synchronize()
+    assert O.rel_l2(qo.cpu().numpy(), ref.legendre_analys(g_ref)) < TOL
+
+
+def test_device_pointer_batch(device):
+    import torch
+    lmax, (nlat, nphi) = 127, gaussGrid(127)
+    plan = make(device, lmax, nlat, nphi)
+    B = 16
+    qs = np.stack([scaled_spectrum(lmax, lmax, b) for b in range(B)])
+    qd = torch.from_numpy(qs).cuda()
+    sd = torch.empty(B, nlat * nphi, device="cuda")
+    qo = torch.empty_like(qd)
+    st = torch.cuda.current_stream().cuda_stream
+    plan.synth_dev(qd.data_ptr(), sd.data_ptr(), B, st)
+    plan.analys_dev(sd.data_ptr(), qo.data_ptr(), B, st)
+    torch.cuda.synchronize()
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    assert O.rel_l2(sd[3].cpu().numpy(), ref.synth(qs[3].astype(np.float64))) < TOL
+    assert O.rel_l2(qo.cpu().numpy(), qs) < TOL
+
+
+def test_errors(device):
+    plan = make(device, 31, 32, 64)
+    with pytest.raises(ValueError, match="qlm must have length"):
+        plan.synth(np.zeros(10, dtype=np.float32))
+    with pytest.raises(ValueError, match="spat must have length"):
+        plan.analys(np.zeros(10, dtype=np.float32))
+    with pytest.raises(ValueError, match="fourier 'fft' requires"):
+        make(device, 31, 32, 100, fourier="fft")
+    with pytest.raises(ValueError, match="nlat must be"):
+        make(device, 31, 31, 64)

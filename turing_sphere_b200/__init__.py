@@ -1,0 +1,8 @@
+"""turing_sphere_b200: B200-native spherical-harmonic transforms and IMEX
+reaction-diffusion steps for turing-sphere's .m models, behind a C ABI
+(include/turing_sht.h, libturing_sht.so)."""
+from .layout import ShtConfig, gaussGrid, gridForLmax, isPowerOfTwo, lmIndex, nlmCalc, validateConfig
+from .sht import Device, ShtPlan, requestShtDevice
+
+__all__ = ["ShtConfig", "gaussGrid", "gridForLmax", "isPowerOfTwo", "lmIndex", "nlmCalc",
+           "validateConfig", "Device", "ShtPlan", "requestShtDevice"]

@@ -1,0 +1,405 @@
+// C ABI entry points: context, layout helpers, SHT plans and transforms.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "runtime.h"
+
+namespace {
+
+int fail(ts_ctx ctx, const ts_exc &e) {
+  ts_set_error(ctx, e.msg);
+  return e.code;
+}
+
+#define TS_API_BEGIN try {
+#define TS_API_END(ctx)                                           \
+  }                                                               \
+  catch (const ts_exc &e) {                                       \
+    return fail(ctx, e);                                          \
+  }                                                               \
+  catch (const std::exception &e) {                               \
+    return fail(ctx, ts_exc{TS_ERR_INVALID, e.what()});           \
+  }                                                               \
+  catch (...) {                                                   \
+    return fail(ctx, ts_exc{TS_ERR_INVALID, "unknown exception"}); \
+  }                                                               \
+  return TS_OK;
+
+thread_local std::string g_noctx_err;
+
+std::string config_error(int lmax, int mmax, int nlat, int nphi) {
+  char buf[256];
+  if (lmax < 1) {
+    snprintf(buf, sizeof buf, "lmax must be an integer >= 1 (got %d)", lmax);
+    return buf;
+  }
+  if (mmax < 0 || mmax > lmax) {
+    snprintf(buf, sizeof buf, "mmax must be an integer in [0, lmax] (got %d)", mmax);
+    return buf;
+  }
+  if (nlat <= lmax) {
+    snprintf(buf, sizeof buf,
+             "nlat must be an integer > lmax for exact Gauss quadrature (got nlat=%d, lmax=%d)",
+             nlat, lmax);
+    return buf;
+  }
+  if (nphi < 2 * mmax + 1) {
+    snprintf(buf, sizeof buf,
+             "nphi must be an integer >= 2*mmax+1 to avoid aliasing (got nphi=%d, mmax=%d)", nphi,
+             mmax);
+    return buf;
+  }
+  return "";
+}
+
+// H = nphi/2 = 2^a 3^b -> Stockham radices (3s first, then 4s, one 2 if a odd)
+bool fft_radices(int nphi, TsFftTab &ft) {
+  if (nphi % 2) return false;
+  int H = nphi / 2, a = 0, b = 0;
+  while (H % 2 == 0) {
+    H /= 2;
+    a++;
+  }
+  while (H % 3 == 0) {
+    H /= 3;
+    b++;
+  }
+  if (H != 1) return false;
+  int n = 0;
+  for (int i = 0; i < b; i++) ft.radix[n++] = 3;
+  for (int i = 0; i < a / 2; i++) ft.radix[n++] = 4;
+  if (a & 1) ft.radix[n++] = 2;
+  if (n > 16) return false;
+  ft.nst = n;
+  return true;
+}
+
+void plan_free(ts_plan p) {
+  for (void *q : {(void *)p->d_x64, (void *)p->d_w64, (void *)p->d_ab64, (void *)p->d_amm64,
+                  (void *)p->d_ct, (void *)p->d_st, (void *)p->d_wq, (void *)p->d_amm,
+                  (void *)p->d_ab, (void *)p->d_tw})
+    if (q) cudaFree(q);
+  p->fm.release();
+  p->stage_q.release();
+  p->stage_s.release();
+}
+
+void check_batch(ts_plan p, const void *a, const void *b, int batch) {
+  TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
+  TS_REQUIRE(a != nullptr && b != nullptr, TS_ERR_INVALID, "null buffer");
+  TS_REQUIRE(batch >= 1 && batch <= 65535, TS_ERR_INVALID, "batch must be in [1, 65535]");
+}
+
+long npts_of(ts_plan p) { return (long)p->nlat * p->nphi; }
+
+void synth_dev(ts_plan p, const float *qlm, float *spat, int batch, cudaStream_t s) {
+  const long fm_stride = (long)(p->mmax + 1) * p->nlat;
+  p->fm.ensure(sizeof(float2) * fm_stride * batch);
+  float2 *fm = (float2 *)p->fm.p;
+  ts_launch_leg_synth(p, (const float2 *)qlm, p->nlm, fm, fm_stride, batch, s);
+  ts_launch_fourier_synth(p, fm, fm_stride, spat, npts_of(p), batch, s);
+}
+
+void analys_dev(ts_plan p, const float *spat, float *qlm, int batch, cudaStream_t s) {
+  const long fm_stride = (long)(p->mmax + 1) * p->nlat;
+  p->fm.ensure(sizeof(float2) * fm_stride * batch);
+  float2 *fm = (float2 *)p->fm.p;
+  ts_launch_fourier_analys(p, spat, npts_of(p), fm, fm_stride, batch, s);
+  ts_launch_leg_analys(p, fm, fm_stride, (float2 *)qlm, p->nlm, batch, s);
+}
+
+}  // namespace
+
+void ts_set_error(ts_ctx ctx, const std::string &msg) {
+  if (ctx)
+    ctx->err = msg;
+  else
+    g_noctx_err = msg;
+}
+
+cudaStream_t ts_pick_stream(ts_ctx ctx, void *stream) {
+  return stream ? (cudaStream_t)stream : ctx->stream;
+}
+
+extern "C" {
+
+// ------------------------------------------------------------------ context
+
+int ts_ctx_create(int device_ordinal, ts_ctx *out) {
+  ts_ctx ctx = nullptr;
+  try {
+    TS_REQUIRE(out != nullptr, TS_ERR_INVALID, "null output handle");
+    int n = 0;
+    TS_CUDA(cudaGetDeviceCount(&n));
+    TS_REQUIRE(device_ordinal >= 0 && device_ordinal < n, TS_ERR_INVALID,
+               "device ordinal out of range");
+    ctx = new ts_ctx_s();
+    ctx->device = device_ordinal;
+    TS_CUDA(cudaSetDevice(device_ordinal));
+    cudaDeviceProp prop;
+    TS_CUDA(cudaGetDeviceProperties(&prop, device_ordinal));
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    ctx->name = prop.name;
+    TS_CUDA(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+    ctx->stream = ctx->own_stream;
+    ts_kernel_attrs_once(ctx);
+    *out = ctx;
+    return TS_OK;
+  } catch (const ts_exc &e) {
+    g_noctx_err = e.msg;
+    if (ctx) {
+      if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+      delete ctx;
+    }
+    return e.code;
+  }
+}
+
+int ts_ctx_destroy(ts_ctx ctx) {
+  if (!ctx) return TS_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->own_stream) {
+    cudaStreamSynchronize(ctx->own_stream);
+    cudaStreamDestroy(ctx->own_stream);
+  }
+  delete ctx;
+  return TS_OK;
+}
+
+const char *ts_last_error(ts_ctx ctx) { return ctx ? ctx->err.c_str() : g_noctx_err.c_str(); }
+
+int ts_ctx_set_stream(ts_ctx ctx, void *stream) {
+  if (!ctx) return TS_ERR_INVALID;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return TS_OK;
+}
+
+void *ts_ctx_stream(ts_ctx ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int ts_ctx_device_name(ts_ctx ctx, char *buf, size_t cap) {
+  if (!ctx || !buf || cap == 0) return TS_ERR_INVALID;
+  snprintf(buf, cap, "%s", ctx->name.c_str());
+  return TS_OK;
+}
+
+int ts_sync(ts_ctx ctx) {
+  TS_API_BEGIN
+  TS_REQUIRE(ctx != nullptr, TS_ERR_INVALID, "null context");
+  TS_CUDA(cudaSetDevice(ctx->device));
+  TS_CUDA(cudaStreamSynchronize(ctx->stream));
+  TS_API_END(ctx)
+}
+
+// ------------------------------------------------------------------- layout
+
+long ts_nlm_calc(int lmax, int mmax) {
+  return (long)(mmax + 1) * (lmax + 1) - (long)mmax * (mmax + 1) / 2;
+}
+
+long ts_lm_index(int lmax, int l, int m) {
+  return (long)m * (lmax + 1) - (long)m * (m - 1) / 2 + (l - m);
+}
+
+int ts_validate_config(int lmax, int mmax, int nlat, int nphi, char *buf, size_t cap) {
+  const std::string e = config_error(lmax, mmax, nlat, nphi);
+  if (buf && cap) snprintf(buf, cap, "%s", e.c_str());
+  return e.empty() ? TS_OK : TS_ERR_INVALID;
+}
+
+void ts_grid_for_lmax(int lmax, int pdeg, int *nlat, int *nphi) {
+  double minlat = ((double)(pdeg + 1) * lmax + 1) / 2.0;
+  if (minlat < lmax + 1) minlat = lmax + 1;
+  *nlat = 2 * (int)std::ceil(minlat / 2.0);
+  int n = 1;
+  while (n < (pdeg + 1) * lmax + 1) n *= 2;
+  *nphi = n;
+}
+
+// --------------------------------------------------------------------- plan
+
+int ts_sht_plan_create(ts_ctx ctx, int lmax, int mmax, int nlat, int nphi, int flags,
+                       ts_plan *out) {
+  ts_plan p = nullptr;
+  try {
+    TS_REQUIRE(ctx != nullptr, TS_ERR_INVALID, "null context");
+    TS_REQUIRE(out != nullptr, TS_ERR_INVALID, "null output handle");
+    const std::string e = config_error(lmax, mmax, nlat, nphi);
+    TS_REQUIRE(e.empty(), TS_ERR_INVALID, e);
+    TS_CUDA(cudaSetDevice(ctx->device));
+    p = new ts_plan_s();
+    p->ctx = ctx;
+    p->lmax = lmax;
+    p->mmax = mmax;
+    p->nlat = nlat;
+    p->nphi = nphi;
+    p->nh = (nlat + 1) / 2;
+    p->nlm = ts_nlm_calc(lmax, mmax);
+    p->precision = flags & TS_PREC_MASK;
+    TS_REQUIRE(p->precision == TS_PREC_FP32 || p->precision == TS_PREC_TF32X3 ||
+                   p->precision == TS_PREC_BF16X3,
+               TS_ERR_INVALID, "unknown precision flag");
+    p->fft.nphi = nphi;
+    p->fft.H = nphi / 2;
+    p->fft.mmax = mmax;
+    p->fft.nlat = nlat;
+    const int want = flags & TS_FOURIER_MASK;
+    const bool fft_ok = fft_radices(nphi, p->fft);
+    if (want == TS_FOURIER_FFT && !fft_ok) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "fourier 'fft' requires nphi = 2^a 3^b with a >= 1 (nphi=%d)", nphi);
+      ts_throw(TS_ERR_INVALID, buf);
+    }
+    p->fourier = (want == TS_FOURIER_DFT || !fft_ok) ? TS_FOURIER_DFT : TS_FOURIER_FFT;
+    if (p->fourier == TS_FOURIER_DFT) p->fft.nst = 0;
+    ts_init_tables(p);
+    if (p->precision != TS_PREC_FP32) {
+      ts_throw(TS_ERR_UNSUPPORTED, "tensor-core precision is not built into this library yet");
+    }
+    *out = p;
+    return TS_OK;
+  } catch (const ts_exc &e) {
+    if (p) {
+      plan_free(p);
+      delete p;
+    }
+    ts_set_error(ctx, e.msg);
+    return e.code;
+  }
+}
+
+int ts_sht_plan_destroy(ts_plan p) {
+  if (!p) return TS_ERR_INVALID;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  plan_free(p);
+  delete p;
+  return TS_OK;
+}
+
+int ts_sht_plan_info(ts_plan p, ts_plan_info *info) {
+  if (!p || !info) return TS_ERR_INVALID;
+  memset(info, 0, sizeof(*info));
+  info->lmax = p->lmax;
+  info->mmax = p->mmax;
+  info->nlat = p->nlat;
+  info->nphi = p->nphi;
+  info->nlm = p->nlm;
+  info->precision = p->precision;
+  info->fourier = p->fourier;
+  info->fft_stages = p->fourier == TS_FOURIER_FFT ? p->fft.nst : 0;
+  for (int i = 0; i < info->fft_stages; i++) info->fft_radix[i] = p->fft.radix[i];
+  return TS_OK;
+}
+
+int ts_sht_plan_nodes(ts_plan p, double *cos_theta, double *weights) {
+  if (!p) return TS_ERR_INVALID;
+  if (cos_theta) memcpy(cos_theta, p->h_x.data(), sizeof(double) * p->nlat);
+  if (weights) memcpy(weights, p->h_w.data(), sizeof(double) * p->nlat);
+  return TS_OK;
+}
+
+// ---------------------------------------------------------------- transforms
+
+int ts_sht_synth_dev(ts_plan p, const float *qlm, float *spat, int batch, void *stream) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, qlm, spat, batch);
+  TS_CUDA(cudaSetDevice(ctx->device));
+  synth_dev(p, qlm, spat, batch, ts_pick_stream(ctx, stream));
+  TS_API_END(ctx)
+}
+
+int ts_sht_analys_dev(ts_plan p, const float *spat, float *qlm, int batch, void *stream) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, spat, qlm, batch);
+  TS_CUDA(cudaSetDevice(ctx->device));
+  analys_dev(p, spat, qlm, batch, ts_pick_stream(ctx, stream));
+  TS_API_END(ctx)
+}
+
+int ts_sht_synth(ts_plan p, const float *qlm, long qlm_len, float *spat, long spat_len,
+                 int batch) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, qlm, spat, batch);
+  char buf[128];
+  snprintf(buf, sizeof buf, "qlm must have length %ld", 2 * p->nlm * batch);
+  TS_REQUIRE(qlm_len == 2 * p->nlm * batch, TS_ERR_SIZE, buf);
+  snprintf(buf, sizeof buf, "spat must have length %ld", npts_of(p) * batch);
+  TS_REQUIRE(spat_len == npts_of(p) * batch, TS_ERR_SIZE, buf);
+  TS_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  p->stage_q.ensure(sizeof(float) * qlm_len);
+  p->stage_s.ensure(sizeof(float) * spat_len);
+  TS_CUDA(cudaMemcpyAsync(p->stage_q.p, qlm, sizeof(float) * qlm_len, cudaMemcpyHostToDevice, s));
+  synth_dev(p, (const float *)p->stage_q.p, (float *)p->stage_s.p, batch, s);
+  TS_CUDA(cudaMemcpyAsync(spat, p->stage_s.p, sizeof(float) * spat_len, cudaMemcpyDeviceToHost, s));
+  TS_CUDA(cudaStreamSynchronize(s));
+  TS_API_END(ctx)
+}
+
+int ts_sht_analys(ts_plan p, const float *spat, long spat_len, float *qlm, long qlm_len,
+                  int batch) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, spat, qlm, batch);
+  char buf[128];
+  snprintf(buf, sizeof buf, "spat must have length %ld", npts_of(p) * batch);
+  TS_REQUIRE(spat_len == npts_of(p) * batch, TS_ERR_SIZE, buf);
+  snprintf(buf, sizeof buf, "qlm must have length %ld", 2 * p->nlm * batch);
+  TS_REQUIRE(qlm_len == 2 * p->nlm * batch, TS_ERR_SIZE, buf);
+  TS_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  p->stage_q.ensure(sizeof(float) * qlm_len);
+  p->stage_s.ensure(sizeof(float) * spat_len);
+  TS_CUDA(cudaMemcpyAsync(p->stage_s.p, spat, sizeof(float) * spat_len, cudaMemcpyHostToDevice, s));
+  analys_dev(p, (const float *)p->stage_s.p, (float *)p->stage_q.p, batch, s);
+  TS_CUDA(cudaMemcpyAsync(qlm, p->stage_q.p, sizeof(float) * qlm_len, cudaMemcpyDeviceToHost, s));
+  TS_CUDA(cudaStreamSynchronize(s));
+  TS_API_END(ctx)
+}
+
+int ts_sht_leg_synth_dev(ts_plan p, const float *qlm, float *fm, int batch, void *stream) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, qlm, fm, batch);
+  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_launch_leg_synth(p, (const float2 *)qlm, p->nlm, (float2 *)fm, (long)(p->mmax + 1) * p->nlat,
+                      batch, ts_pick_stream(ctx, stream));
+  TS_API_END(ctx)
+}
+
+int ts_sht_fourier_synth_dev(ts_plan p, const float *fm, float *spat, int batch, void *stream) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, fm, spat, batch);
+  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_launch_fourier_synth(p, (const float2 *)fm, (long)(p->mmax + 1) * p->nlat, spat, npts_of(p),
+                          batch, ts_pick_stream(ctx, stream));
+  TS_API_END(ctx)
+}
+
+int ts_sht_fourier_analys_dev(ts_plan p, const float *spat, float *fm, int batch, void *stream) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, spat, fm, batch);
+  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_launch_fourier_analys(p, spat, npts_of(p), (float2 *)fm, (long)(p->mmax + 1) * p->nlat,
+                           batch, ts_pick_stream(ctx, stream));
+  TS_API_END(ctx)
+}
+
+int ts_sht_leg_analys_dev(ts_plan p, const float *fm, float *qlm, int batch, void *stream) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, fm, qlm, batch);
+  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_launch_leg_analys(p, (const float2 *)fm, (long)(p->mmax + 1) * p->nlat, (float2 *)qlm,
+                       p->nlm, batch, ts_pick_stream(ctx, stream));
+  TS_API_END(ctx)
+}
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+// Shared device helpers for the turing-sphere SHT kernels.
+//
+// Every header under kernels/ is compiled twice: by nvcc into the library
+// (standalone transforms) and by NVRTC at model-compile time together with
+// the generated reaction / IMEX code.  So: no #include of system headers, no
+// std::, only CUDA builtins.
+#pragma once
+
+#define TS_DEV __device__ __forceinline__
+
+// fp32 extended-range recurrence constants (common.ts:17-20 of the
+// reference: SCALE = 2^56, ACCURACY = 1e-15, rescale threshold
+// ACCURACY*SCALE + 1).  A per-latitude integer exponent `ny` counts the
+// factors of SCALE carried by the running Legendre value; a term contributes
+// only once ny == 0.
+#define TS_SCALE 72057594037927936.0f
+#define TS_INV_SCALE 1.387778780781445675529539585113525390625e-17f
+#define TS_ACCURACY 1e-15f
+#define TS_RESCALE_THR (TS_ACCURACY * TS_SCALE + 1.0f)
+
+TS_DEV float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+TS_DEV float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+TS_DEV float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+TS_DEV float2 c_mul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+TS_DEV float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+// multiply by +i / -i
+TS_DEV float2 c_mul_i(float2 a) { return make_float2(-a.y, a.x); }
+TS_DEV float2 c_mul_negi(float2 a) { return make_float2(a.y, -a.x); }
+
+// lm index of (l = m, m) in m-major order (layout.ts:30-32).
+TS_DEV long ts_lm_base(int lmax, int m) {
+  return (long)m * (lmax + 1) - ((long)m * (m - 1)) / 2;
+}
+
+// sin(theta)^m with an extended exponent: returns y and ny such that the
+// value is y * SCALE^ny (ny <= 0), y kept above ~ACCURACY.  Binary
+// exponentiation over the bits of m; the running power s = st^(2^k) carries
+// its own exponent ns and is renormalised whenever it drops below 1/SCALE.
+TS_DEV void ts_sinpow(float st, int m, float &y, int &ny) {
+  y = 1.0f;
+  ny = 0;
+  float s = st;
+  int ns = 0;
+  int bits = m;
+  while (bits) {
+    if (bits & 1) {
+      y *= s;
+      ny += ns;
+      if (y < TS_ACCURACY + TS_INV_SCALE) {
+        y *= TS_SCALE;
+        ny -= 1;
+      }
+    }
+    bits >>= 1;
+    if (!bits) break;
+    s *= s;
+    ns += ns;
+    if (s < TS_INV_SCALE) {
+      s *= TS_SCALE;
+      ns -= 1;
+    }
+  }
+}
+
+// Read-only parameters of one transform plan as the kernels see them.
+struct TsLegTab {
+  const float *ct;   // cos(theta) of the northern latitudes (nh entries)
+  const float *st;   // sin(theta)
+  const float *wq;   // Gauss weight * 2*pi/nphi
+  const float2 *ab;  // (a_l^m, b_l^m) per lm
+  const float *amm;  // seed amplitude per m (Condon-Shortley sign included)
+  int lmax, mmax, nlat, nh;  // nh = ceil(nlat/2): latitudes a recurrence walks
+};
+
+struct TsFftTab {
+  const float2 *tw;  // (cos, sin)(2*pi*k/nphi), k < nphi
+  int nphi, H, mmax, nlat;
+  int nst;           // Stockham stages of the H-point complex FFT
+  int radix[16];
+};

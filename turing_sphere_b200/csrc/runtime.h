@@ -1,0 +1,95 @@
+// Internal runtime types of libturing_sht.so (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/turing_sht.h"
+#include "kernels/ts_common.cuh"
+
+struct ts_exc {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] inline void ts_throw(int code, const std::string &msg) { throw ts_exc{code, msg}; }
+
+#define TS_CUDA(call)                                                                \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      ts_throw(TS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+#define TS_REQUIRE(cond, code, msg) \
+  do {                              \
+    if (!(cond)) ts_throw(code, msg); \
+  } while (0)
+
+struct ts_ctx_s {
+  int device = 0;
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::string name;
+};
+
+// Device buffer with grow-on-demand capacity (bytes).
+struct ts_dbuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    TS_CUDA(cudaMalloc(&p, bytes));
+    cap = bytes;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct ts_plan_s {
+  ts_ctx ctx = nullptr;
+  int lmax = 0, mmax = 0, nlat = 0, nphi = 0, nh = 0;
+  long nlm = 0;
+  int precision = TS_PREC_FP32;
+  int fourier = TS_FOURIER_FFT;
+  // FP64 nodes/weights as computed on the GPU, host copies
+  std::vector<double> h_x, h_w;
+  // device tables
+  double *d_x64 = nullptr, *d_w64 = nullptr, *d_ab64 = nullptr, *d_amm64 = nullptr;
+  float *d_ct = nullptr, *d_st = nullptr, *d_wq = nullptr, *d_amm = nullptr;
+  float2 *d_ab = nullptr, *d_tw = nullptr;
+  TsLegTab leg{};
+  TsFftTab fft{};
+  // scratch: fm intermediate, host-call staging
+  ts_dbuf fm, stage_q, stage_s;
+  // tensor-core tables (precision != FP32)
+  void *tc = nullptr;
+};
+
+cudaStream_t ts_pick_stream(ts_ctx ctx, void *stream);
+void ts_set_error(ts_ctx ctx, const std::string &msg);
+
+// launchers (sht_kernels.cu)
+void ts_launch_leg_synth(ts_plan p, const float2 *q, long q_stride, float2 *fm, long fm_stride,
+                         int nfields, cudaStream_t s);
+void ts_launch_leg_analys(ts_plan p, const float2 *g, long g_stride, float2 *q, long q_stride,
+                          int nfields, cudaStream_t s);
+void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fm_stride, float *spat,
+                             long spat_stride, int nfields, cudaStream_t s);
+void ts_launch_fourier_analys(ts_plan p, const float *spat, long spat_stride, float2 *g,
+                              long g_stride, int nfields, cudaStream_t s);
+void ts_init_tables(ts_plan p);
+void ts_kernel_attrs_once(ts_ctx ctx);
