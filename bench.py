@@ -203,7 +203,10 @@ def main():
     lmax, B = args.lmax, args.batch
     nlat, nphi = grid(lmax)
     dev = Device(local)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: torch's default current stream is the legacy NULL
+    # stream, which the C ABI reads as "the context's own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     dev.set_stream(stream.cuda_stream)
     plan = ShtPlan.create(dev, ShtConfig(lmax, lmax, nlat, nphi), {"precision": args.precision})
     nlm = plan.nlm
