@@ -114,6 +114,19 @@ int ts_sht_plan_nodes(ts_plan plan, double *cos_theta, double *weights);
 int ts_sht_synth_dev(ts_plan plan, const float *qlm, float *spat, int batch, void *stream);
 int ts_sht_analys_dev(ts_plan plan, const float *spat, float *qlm, int batch, void *stream);
 
+/* Allocation-free synthesis.  No counterpart in the reference: it exists for
+ * callers that cannot let the library call cudaMalloc (hosts that own every
+ * device allocation, or loops that must not stall on cudaMalloc's implicit
+ * device synchronisation).  Same inputs, outputs and result as
+ * ts_sht_synth_dev, but the Fourier intermediate lives in a fixed 16 MiB
+ * array compiled into the library (held on every GPU that loads it until the
+ * process exits), so the call allocates nothing.  A batch whose intermediate
+ * exceeds 16 MiB ((mmax+1)*nlat*8 bytes per field) fails with TS_ERR_SIZE.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the one array: calls
+ * that overlap on the GPU (different streams, no ordering) race. */
+int ts_sht_synth_noalloc(ts_plan plan, const float *qlm, float *spat, int batch, void *stream);
+
 /* Blocking transforms on host arrays (ShtPlan.synth / ShtPlan.analys,
  * sht.ts:414-461); they fail with TS_ERR_SIZE on a length mismatch. */
 int ts_sht_synth(ts_plan plan, const float *qlm, long qlm_len, float *spat, long spat_len,

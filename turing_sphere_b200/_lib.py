@@ -83,6 +83,7 @@ SIGNATURES = {
     "ts_sht_plan_nodes": (i32, [vp, f64p, f64p]),
     "ts_sht_synth_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_analys_dev": (i32, [vp, vp, vp, i32, vp]),
+    "ts_sht_synth_noalloc": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_synth": (i32, [vp, f32p, i64, f32p, i64, i32]),
     "ts_sht_analys": (i32, [vp, f32p, i64, f32p, i64, i32]),
     "ts_sht_leg_synth_dev": (i32, [vp, vp, vp, i32, vp]),
