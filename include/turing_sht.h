@@ -143,6 +143,88 @@ int ts_sht_fourier_analys_dev(ts_plan plan, const float *spat, float *fm, int ba
                               void *stream);
 int ts_sht_leg_analys_dev(ts_plan plan, const float *fm, float *qlm, int batch, void *stream);
 
+/* --------------------------------------------------------------- models
+ * A .m model (init/step functions, src/mgpu/model.ts:1-19) compiled for a
+ * plan's grid: parsed and specialised (src/mgpu/compile.ts:83-190), every
+ * element-wise statement emitted as CUDA C and compiled by NVRTC for sm_100a,
+ * with the grid statements fused between the synthesis and analysis FFTs and
+ * the spectral statements after an analysis fused into its Legendre epilogue.
+ * The host bindings a .m may name are those of model.ts:116-125: lam
+ * (l(l+1), 2 x nlm), noise (npts x 1), npts, nlm, the state names (2 x nlm)
+ * and the parameter names (runtime scalars: changing one rewrites a small
+ * buffer and recompiles nothing, compile.ts:34-40).  `batch` independent
+ * instances advance together; each has its own state, noise and parameters. */
+typedef struct ts_compile_error {
+  long start, end; /* byte offsets into the source, -1 when unknown */
+  char fn[64];     /* function being compiled ("init", "step") */
+  char message[1024];
+} ts_compile_error;
+
+/* GpuModel.create (model.ts:103-163).  Returns TS_ERR_COMPILE with `err`
+ * filled (ModelCompileError / UnsupportedOnGpu, errors.ts:14-31) when the
+ * source is rejected. */
+int ts_model_compile(ts_plan plan, const char *source, const char *const *state, int nstate,
+                     const char *const *view, int nview, const char *const *params, int nparams,
+                     int batch, ts_model *out, ts_compile_error *err);
+int ts_model_destroy(ts_model model);
+
+/* ModelPlan.setParams (plan.ts:410-420): values in the model's parameter
+ * order, the same for every instance; non-finite values become 0. */
+int ts_model_set_params(ts_model model, const float *values, int n);
+/* Per-instance parameters: values[batch][n] (a parameter sweep). */
+int ts_model_set_params_batched(ts_model model, const float *values, int batch, int n);
+
+/* GpuModel.upload (plan.ts:77-86): a host-owned value (a state, noise, lam)
+ * from host memory; n = one instance's length (copied to every instance) or
+ * batch times it.  TS_ERR_NOT_FOUND for an unknown name, TS_ERR_SIZE for a
+ * wrong length. */
+int ts_model_upload(ts_model model, const char *name, const float *data, long n);
+
+/* GpuModel.init (model.ts:180-186): upload the seeded perturbation (may be
+ * NULL to keep the current one) and run `init`.  Asynchronous. */
+int ts_model_init(ts_model model, const float *noise, long n);
+/* GpuModel.step (model.ts:229-234): `nsteps` timesteps.  Asynchronous. */
+int ts_model_step(ts_model model, int nsteps);
+
+/* GpuModel.read (model.ts:262-277): blocking read of a named value — from the
+ * function that ran most recently, as #locate does (model.ts:243-252).
+ * n = batch x length (all instances) or length (instance 0). */
+int ts_model_read(ts_model model, const char *name, float *out, long n);
+/* GpuModel.valueBuffer (model.ts:254-259): the device buffer of a named value
+ * ([batch][count] floats; stride 0 for values shared by all instances). */
+int ts_model_value_ptr(ts_model model, const char *name, float **dev, long *count);
+
+/* snapshotState / restoreState (model.ts:195-223). */
+int ts_model_snapshot(ts_model model);
+int ts_model_restore(ts_model model);
+
+/* GpuModel.describe (plan.ts:486-488): the statements each function compiled
+ * to and the launches that run them; which = 0 (init) or 1 (step). */
+int ts_model_describe(ts_model model, int which, char *buf, size_t cap);
+/* The generated CUDA C of both functions. */
+int ts_model_source(ts_model model, char *buf, size_t cap);
+/* Element-wise statements (the reference's kernel count, the fusion guard of
+ * test/modelChecks.ts:17-21) and launches per call. */
+int ts_model_counts(ts_model model, int which, int *kernels, int *launches);
+
+/* Everything ts_model_compile does short of the GPU — parse, specialise,
+ * schedule, generate CUDA C and compile it with NVRTC for sm_100a — for a grid
+ * given by its sizes (no context, no device).  `describe` receives the
+ * describe() text of init and step separated by a "====" line; `kernels` and
+ * `launches` are those of step.  For host-side checks of a model source
+ * (the editor's compile-on-type, src/editor/, and the tests). */
+int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
+                   const char *const *state, int nstate, const char *const *view, int nview,
+                   const char *const *params, int nparams, int batch, char *describe,
+                   size_t cap, int *kernels, int *launches, ts_compile_error *err);
+
+/* Seeding (src/mgpu/noise.ts:15-51; bench-sht.ts:132-144): mulberry32 and
+ * Box-Muller, bit-identical integer state to the reference's.  amp-scaled
+ * normals per grid point, and a uniform [-1, 1) spectrum with m = 0 imaginary
+ * parts zero. */
+void ts_seeded_noise(long npts, double amp, unsigned seed, float *out);
+void ts_seeded_spectrum(int lmax, int mmax, unsigned seed, float *qlm);
+
 #ifdef __cplusplus
 }
 #endif

@@ -90,6 +90,26 @@ SIGNATURES = {
     "ts_sht_fourier_synth_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_fourier_analys_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_leg_analys_dev": (i32, [vp, vp, vp, i32, vp]),
+    "ts_model_compile": (i32, [vp, cstr, C.POINTER(cstr), i32, C.POINTER(cstr), i32,
+                               C.POINTER(cstr), i32, i32, C.POINTER(vp), C.POINTER(CompileError)]),
+    "ts_model_destroy": (i32, [vp]),
+    "ts_model_set_params": (i32, [vp, f32p, i32]),
+    "ts_model_set_params_batched": (i32, [vp, f32p, i32, i32]),
+    "ts_model_upload": (i32, [vp, cstr, f32p, i64]),
+    "ts_model_init": (i32, [vp, f32p, i64]),
+    "ts_model_step": (i32, [vp, i32]),
+    "ts_model_read": (i32, [vp, cstr, f32p, i64]),
+    "ts_model_value_ptr": (i32, [vp, cstr, C.POINTER(vp), C.POINTER(i64)]),
+    "ts_model_snapshot": (i32, [vp]),
+    "ts_model_restore": (i32, [vp]),
+    "ts_model_describe": (i32, [vp, i32, C.c_char_p, C.c_size_t]),
+    "ts_model_source": (i32, [vp, C.c_char_p, C.c_size_t]),
+    "ts_model_counts": (i32, [vp, i32, C.POINTER(i32), C.POINTER(i32)]),
+    "ts_model_check": (i32, [i32, i32, i32, i32, cstr, C.POINTER(cstr), i32, C.POINTER(cstr), i32,
+                             C.POINTER(cstr), i32, i32, C.c_char_p, C.c_size_t, C.POINTER(i32),
+                             C.POINTER(i32), C.POINTER(CompileError)]),
+    "ts_seeded_noise": (None, [i64, C.c_double, C.c_uint, f32p]),
+    "ts_seeded_spectrum": (None, [i32, i32, C.c_uint, f32p]),
 }
 
 _lib = None
@@ -116,6 +136,13 @@ def check(status: int, ctx=None) -> None:
     if status != TS_OK:
         msg = lib().ts_last_error(ctx)
         raise TsError(status, (msg or b"").decode() or STATUS_NAMES.get(status, str(status)))
+
+
+def cstr_array(names):
+    arr = (cstr * max(1, len(names)))()
+    for i, n in enumerate(names):
+        arr[i] = n.encode()
+    return arr
 
 
 def fptr(a):

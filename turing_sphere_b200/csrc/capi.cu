@@ -1,6 +1,7 @@
 // C ABI entry points: context, layout helpers, SHT plans and transforms.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 
 #include "runtime.h"
@@ -403,3 +404,51 @@ int ts_sht_leg_analys_dev(ts_plan p, const float *fm, float *qlm, int batch, voi
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------- seeding
+// mulberry32 uniform deviates and Box-Muller normals with a spare (the
+// generators of src/mgpu/noise.ts:15-51): integer state, then one division
+// by 2^32, so any faithful implementation draws the same sequence.
+namespace {
+struct Mulberry {
+  uint32_t s;
+  bool have = false;
+  double spare = 0;
+  double uniform() {
+    s += 0x6d2b79f5u;
+    uint32_t t = s;
+    t = (t ^ (t >> 15)) * (t | 1u);
+    t ^= t + (t ^ (t >> 7)) * (t | 61u);
+    return (double)(t ^ (t >> 14)) / 4294967296.0;
+  }
+  double normal() {
+    if (have) {
+      have = false;
+      return spare;
+    }
+    double u = 0;
+    while (u == 0) u = uniform();
+    const double r = std::sqrt(-2.0 * std::log(u));
+    const double th = 2.0 * M_PI * uniform();
+    spare = r * std::sin(th);
+    have = true;
+    return r * std::cos(th);
+  }
+};
+}  // namespace
+
+extern "C" void ts_seeded_noise(long npts, double amp, unsigned seed, float *out) {
+  Mulberry g{seed};
+  for (long i = 0; i < npts; i++) out[i] = (float)(amp * g.normal());
+}
+
+extern "C" void ts_seeded_spectrum(int lmax, int mmax, unsigned seed, float *qlm) {
+  Mulberry g{seed};
+  long lm = 0;
+  for (int m = 0; m <= mmax; m++)
+    for (int l = m; l <= lmax; l++, lm++) {
+      qlm[2 * lm] = (float)(2.0 * g.uniform() - 1.0);
+      const float im = (float)(2.0 * g.uniform() - 1.0);
+      qlm[2 * lm + 1] = m == 0 ? 0.0f : im;
+    }
+}

@@ -203,3 +203,101 @@ ts_fourier_analys(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
   __syncthreads();
   ts_store_tile(tile, g + f * g_stride, lat0, LB, ft);
 }
+
+// ------------------------------------------------------- fused grid phase
+//
+// One launch runs a whole grid phase of a compiled model for a block of LB
+// latitude rows of one instance: the synthesis FFTs of the phase's NSYN
+// spectral inputs, the generated element-wise program at every grid point
+// (Prog::eval: reaction terms and any other grid statement), and the analysis
+// FFTs of its NANA outputs.  The grid values live in shared memory and
+// registers only; a grid variable reaches HBM only when it is materialised
+// (NGOUT outputs: a displayed field, or a value a later phase reads).
+//
+//   fm [inst][NSYN][mmax+1][nlat]   -> rows -> eval -> rows -> gm [inst][NANA][mmax+1][nlat]
+
+
+template <class Prog>
+__global__ void __launch_bounds__(512) ts_fourier_phase(TsFftTab ft, TsPhaseIO io) {
+  constexpr int NSYN = Prog::NSYN, NGIN = Prog::NGIN, NANA = Prog::NANA, NGOUT = Prog::NGOUT;
+  constexpr int NR = NSYN + NANA + 1;  // rows per warp: inputs, outputs, one ping-pong row
+  extern __shared__ float2 ts_smem_fp[];
+  const int LB = blockDim.x >> 5;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lat0 = blockIdx.x * LB;
+  const long inst = blockIdx.y;
+  const int lat = lat0 + w;
+  const bool live = lat < ft.nlat;
+  float2 *stw = ts_four_tw(ts_smem_fp);
+  float2 *tile = ts_four_tile(ts_smem_fp, ft);
+  float2 *rowbase = ts_four_rows(ts_smem_fp, ft, LB) + (long)w * NR * ft.H;
+  float2 *rp[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) rp[r] = rowbase + (long)r * ft.H;
+  ts_load_tw(stw, ft);
+
+  // synthesis of every spectral input of the phase
+#pragma unroll
+  for (int s = 0; s < NSYN; s++) {
+    __syncthreads();
+    ts_load_tile(tile, io.fm + (inst * NSYN + s) * io.field, lat0, LB, ft);
+    __syncthreads();
+    if (live) {
+      ts_pack_synth(rp[s], tile, LB, w, stw, ft, lane);
+      const float2 *z = ts_fft_row<+1>(rp[s], rp[NR - 1], stw, ft, lane);
+      if (z != rp[s]) {
+        float2 *tmp = rp[s];
+        rp[s] = rp[NR - 1];
+        rp[NR - 1] = tmp;
+      }
+    }
+  }
+
+  // the element-wise program, two grid points (one packed complex) at a time
+  if (live) {
+    const float *prm = io.prm + inst * io.nprm;
+    const long rowoff = (long)lat * ft.nphi;
+    for (int j = lane; j < ft.H; j += 32) {
+      float in0[NSYN + NGIN > 0 ? NSYN + NGIN : 1], in1[NSYN + NGIN > 0 ? NSYN + NGIN : 1];
+#pragma unroll
+      for (int s = 0; s < NSYN; s++) {
+        const float2 z = rp[s][j];
+        in0[s] = z.x;
+        in1[s] = z.y;
+      }
+#pragma unroll
+      for (int gi = 0; gi < NGIN; gi++) {
+        const float2 x = *reinterpret_cast<const float2 *>(io.gin[gi] + inst * io.gin_stride[gi] +
+                                                           rowoff + 2 * j);
+        in0[NSYN + gi] = x.x;
+        in1[NSYN + gi] = x.y;
+      }
+      float out0[NANA + NGOUT > 0 ? NANA + NGOUT : 1], out1[NANA + NGOUT > 0 ? NANA + NGOUT : 1];
+      Prog::eval(in0, out0, prm);
+      Prog::eval(in1, out1, prm);
+#pragma unroll
+      for (int k = 0; k < NANA; k++) rp[NSYN + k][j] = make_float2(out0[k], out1[k]);
+#pragma unroll
+      for (int o = 0; o < NGOUT; o++)
+        *reinterpret_cast<float2 *>(io.gout[o] + inst * io.gout_stride[o] + rowoff + 2 * j) =
+            make_float2(out0[NANA + o], out1[NANA + o]);
+    }
+  }
+
+  // analysis of every output of the phase
+#pragma unroll
+  for (int k = 0; k < NANA; k++) {
+    if (live) {
+      const float2 *Z = ts_fft_row<-1>(rp[NSYN + k], rp[NR - 1], stw, ft, lane);
+      if (Z != rp[NSYN + k]) {
+        float2 *tmp = rp[NSYN + k];
+        rp[NSYN + k] = rp[NR - 1];
+        rp[NR - 1] = tmp;
+      }
+      ts_unpack_analys(rp[NSYN + k], tile, LB, w, stw, ft, lane);
+    }
+    __syncthreads();
+    ts_store_tile(tile, io.gm + (inst * NANA + k) * io.field, lat0, LB, ft);
+    __syncthreads();
+  }
+}

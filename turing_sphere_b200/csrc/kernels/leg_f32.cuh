@@ -21,8 +21,7 @@
 // Dynamic shared memory: (K + K*F) float2, K = lmax - m + 1 <= lmax + 1.
 template <int F>
 __global__ void __launch_bounds__(128)
-ts_leg_synth_f32(TsLegTab t, const float2 *__restrict__ q, long q_stride,
-                 float2 *__restrict__ fm, long fm_stride, int nfields) {
+ts_leg_synth_f32(TsLegTab t, TsFields q, float2 *__restrict__ fm, long fm_stride, int nfields) {
   extern __shared__ float2 ts_smem_ls[];
   const int m = blockIdx.y;
   const int f0 = blockIdx.z * F;
@@ -34,7 +33,7 @@ ts_leg_synth_f32(TsLegTab t, const float2 *__restrict__ q, long q_stride,
 #pragma unroll
   for (int f = 0; f < F; f++) {
     const bool ok = f0 + f < nfields;
-    const float2 *src = q + (long)(f0 + f) * q_stride + base;
+    const float2 *src = ok ? ts_field(q, f0 + f) + base : nullptr;
     for (int i = threadIdx.x; i < K; i += blockDim.x)
       sq[i * F + f] = ok ? src[i] : make_float2(0.f, 0.f);
   }
@@ -147,16 +146,17 @@ struct TsAnalysStore {
   }
 };
 
+// per_cta <= F fields per CTA (a model groups whole instances per CTA).
 template <int F, int K, int P, class Epi>
 __global__ void __launch_bounds__(256)
 ts_leg_analys_f32(TsLegTab t, const float2 *__restrict__ g, long g_stride, Epi epi,
-                  int nfields) {
+                  int nfields, int per_cta) {
   constexpr int N = 4 * P * F;  // (p, comp4, f) values per span
   constexpr int CNT = N >= 32 ? N / 32 : 1;
   extern __shared__ float ts_smem_la[];
   const int m = blockIdx.x;
-  const int f0 = blockIdx.y * F;
-  const int nf = min(F, nfields - f0);
+  const int f0 = blockIdx.y * per_cta;
+  const int nf = min(per_cta, nfields - f0);
   const int Km = t.lmax - m + 1;
   const long base = ts_lm_base(t.lmax, m);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

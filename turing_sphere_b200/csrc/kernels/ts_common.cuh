@@ -74,9 +74,60 @@ struct TsLegTab {
   int lmax, mmax, nlat, nh;  // nh = ceil(nlat/2): latitudes a recurrence walks
 };
 
+// A set of coefficient fields read by the Legendre synthesis: field f is
+// species s = f % nper of instance i = f / nper, at base[s] + i*inst_stride[s].
+#define TS_MAXIO 8
+struct TsFields {
+  const float2 *base[TS_MAXIO];
+  long inst_stride[TS_MAXIO];
+  int nper;
+};
+
+TS_DEV const float2 *ts_field(const TsFields &q, int f) {
+  const int s = f % q.nper;
+  return q.base[s] + (long)(f / q.nper) * q.inst_stride[s];
+}
+
 struct TsFftTab {
   const float2 *tw;  // (cos, sin)(2*pi*k/nphi), k < nphi
   int nphi, H, mmax, nlat;
   int nst;           // Stockham stages of the H-point complex FFT
   int radix[16];
 };
+
+// Grid-phase I/O of a compiled model (see ts_fourier_phase in fourier.cuh).
+struct TsPhaseIO {
+  const float2 *fm;
+  float2 *gm;
+  long field;  // (mmax+1)*nlat complex values per field
+  const float *gin[TS_MAXIO];
+  long gin_stride[TS_MAXIO];  // per instance (0 = shared by all instances)
+  float *gout[TS_MAXIO];
+  long gout_stride[TS_MAXIO];
+  const float *prm;
+  int nprm;
+};
+
+// Spectral-side I/O of a compiled model's generated code: inputs and outputs
+// are [instance][2*nlm] float arrays (instance stride 0 = shared by all).
+struct TsSpecIO {
+  const float *sin[TS_MAXIO];
+  long sin_stride[TS_MAXIO];
+  float *sout[TS_MAXIO];
+  long sout_stride[TS_MAXIO];
+  const float *prm;
+  int nprm;
+  long n;  // 2*nlm
+};
+
+// x^k by repeated multiplication, left to right (x.^k with a literal integer
+// exponent; a general pow() is undefined for a negative base).
+TS_DEV float ts_pow_i1(float x) { return x; }
+TS_DEV float ts_pow_i2(float x) { return x * x; }
+TS_DEV float ts_pow_i3(float x) { return x * x * x; }
+TS_DEV float ts_pow_i4(float x) { return x * x * x * x; }
+TS_DEV float ts_pow_i5(float x) { return x * x * x * x * x; }
+TS_DEV float ts_pow_i6(float x) { return x * x * x * x * x * x; }
+TS_DEV float ts_pow_i7(float x) { return x * x * x * x * x * x * x; }
+TS_DEV float ts_pow_i8(float x) { return x * x * x * x * x * x * x * x; }
+TS_DEV float ts_sign(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }

@@ -1,0 +1,1112 @@
+// Compiled .m models: scheduling into fused launches, CUDA-C generation,
+// NVRTC compilation for sm_100a, and execution.
+//
+// The reference turns every element-wise statement into one WGSL kernel and
+// every synth/analys into two dispatches, round-tripping each grid field
+// through memory (src/mgpu/plan.ts:287-478, src/mgpu/wgsl.ts:321-372).  Here
+// a function is cut into phases:
+//   LegSynth   the Legendre synthesis of every spectral value the phase reads
+//   Phase      one generated kernel per latitude block: synthesis FFTs, the
+//              phase's grid statements (the reaction) at every point, and the
+//              analysis FFTs of the values passed to analys
+//   LegAnalys  the Legendre analysis, with the spectral statements that
+//              consume its results (the IMEX update) as its epilogue
+//   SpecEW     spectral statements that depend on no analysis in flight
+// Grid values stay on chip; only displayed fields and values a later phase
+// reads are written out.  State outputs go to a second buffer per state and
+// the two swap after the run (the feedback copies of plan.ts:256-281).
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+
+#include "kernel_sources.h"
+#include "mlang.h"
+#include "runtime.h"
+
+using tsm::Dom;
+
+namespace {
+
+struct HostBuf {
+  Dom dom;
+  long count = 0;       // floats per instance
+  bool shared = false;  // one copy for all instances (stride 0)
+  bool state = false;
+  float *cur = nullptr, *next = nullptr;
+};
+
+// where a value lives
+struct Ref {
+  enum K { None, Cur, Next, Plan } k = None;
+  std::string host;
+  int pbuf = -1;
+};
+
+struct Stage {
+  enum Kind { SpecEW, LegSynth, Phase, LegAnalys } kind;
+  std::string expr;  // kernel name expression (NVRTC)
+  cudaKernel_t kern = nullptr;
+  std::vector<Ref> in, out;
+  int nsyn = 0, nana = 0;
+  int lb = 0, F = 1, K = 1, W = 1, per_cta = 1;
+  size_t smem = 0;
+  std::string label;  // one line, for describe()
+  std::string src;    // generated CUDA of this stage
+};
+
+struct Program {
+  tsm::Function fn;
+  std::vector<Stage> stages;
+  std::vector<std::string> feedback;             // per output: state name or ""
+  std::map<std::string, Ref> value_ref;           // readable values after a run
+  std::map<std::string, std::string> lazy_views;  // view -> state it is synth() of
+  std::vector<long> pcount;                       // plan buffer sizes (per instance)
+  std::vector<float *> pbuf;
+  std::set<std::string> swaps;                    // states this program recomputes
+  int nsyn_max = 0, nana_max = 0;
+};
+
+long dom_count(Dom d, ts_plan p) {
+  return d == Dom::Grid ? (long)p->nlat * p->nphi : 2 * p->nlm;
+}
+
+// ------------------------------------------------------------- code emitters
+
+std::string flit(double v) {
+  if (!std::isfinite(v)) throw tsm::CompileError{"cannot emit a non-finite literal"};
+  const float f = (float)v;
+  if (!std::isfinite(f)) throw tsm::CompileError{"literal out of float range"};
+  char buf[64];
+  snprintf(buf, sizeof buf, "%.9g", (double)f);
+  std::string s = buf;
+  if (s.find_first_of(".en") == std::string::npos) s += ".0";
+  return s + "f";
+}
+
+const std::map<std::string, std::string> kCudaFn = {
+    {"abs", "fabsf"},   {"acos", "acosf"},   {"asin", "asinf"}, {"atan", "atanf"},
+    {"atan2", "atan2f"}, {"ceil", "ceilf"},  {"cos", "cosf"},   {"cosh", "coshf"},
+    {"exp", "expf"},    {"floor", "floorf"}, {"log", "logf"},   {"log2", "log2f"},
+    {"max", "fmaxf"},   {"min", "fminf"},    {"round", "roundf"}, {"sign", "ts_sign"},
+    {"sin", "sinf"},    {"sinh", "sinhf"},   {"sqrt", "sqrtf"}, {"tan", "tanf"},
+    {"tanh", "tanhf"}};
+
+struct Emitter {
+  const tsm::Function &f;
+  std::map<int, std::string> name;  // var id -> C expression
+
+  std::string e(const tsm::ExprP &x) {
+    switch (x->kind) {
+      case tsm::Expr::Lit: return flit(x->value);
+      case tsm::Expr::Fill: return flit(x->value);
+      case tsm::Expr::Param: return "prm[" + std::to_string(x->index) + "]";
+      case tsm::Expr::Scalar: return "s" + std::to_string(x->index);
+      case tsm::Expr::Var: {
+        auto it = name.find(x->index);
+        if (it == name.end())
+          throw tsm::CompileError{"internal: value '" + f.vars[x->index].name + "' not bound"};
+        return it->second;
+      }
+      case tsm::Expr::Binary: return "(" + e(x->args[0]) + " " + x->op + " " + e(x->args[1]) + ")";
+      case tsm::Expr::Unary: return "(-" + e(x->args[0]) + ")";
+      case tsm::Expr::PowI: {
+        const int k = x->k < 0 ? -x->k : x->k;
+        const std::string b = "ts_pow_i" + std::to_string(k) + "(" + e(x->args[0]) + ")";
+        return x->k < 0 ? "(1.0f / " + b + ")" : b;
+      }
+      case tsm::Expr::Call: {
+        std::string s = kCudaFn.at(x->fn) + "(";
+        for (size_t i = 0; i < x->args.size(); i++) s += (i ? ", " : "") + e(x->args[i]);
+        return s + ")";
+      }
+    }
+    return "0.0f";
+  }
+
+  // derived scalars, in definition order (they only read params and earlier scalars)
+  std::string scalars() {
+    std::string s;
+    for (size_t i = 0; i < f.scalars.size(); i++)
+      s += "  const float s" + std::to_string(i) + " = " + e(f.scalars[i].expr) + ";\n";
+    return s;
+  }
+};
+
+void collect_vars(const tsm::ExprP &x, std::set<int> &out) {
+  if (x->kind == tsm::Expr::Var) out.insert(x->index);
+  for (auto &a : x->args) collect_vars(a, out);
+}
+
+std::vector<int> stmt_inputs(const tsm::Stmt &s) {
+  if (s.kind != tsm::Stmt::Elementwise) return {s.arg};
+  std::set<int> v;
+  collect_vars(s.expr, v);
+  return std::vector<int>(v.begin(), v.end());
+}
+
+}  // namespace
+
+struct ts_model_s {
+  ts_ctx ctx = nullptr;
+  ts_plan plan = nullptr;
+  int batch = 1;
+  std::vector<std::string> state, view, params;
+  std::map<std::string, HostBuf> host;
+  Program prog[2];  // init, step
+  float *d_prm = nullptr;
+  std::vector<float> h_prm;
+  ts_dbuf fm, gm, stash;
+  cudaLibrary_t lib = nullptr;
+  int last_ran = 0, stashed_ran = 0;
+  std::string source;
+  std::vector<float *> owned;
+};
+
+namespace {
+
+// ------------------------------------------------------------------ scheduler
+
+void schedule(ts_model m, Program &P, bool is_step) {
+  const tsm::Function &f = P.fn;
+  ts_plan p = m->plan;
+  const int nv = (int)f.vars.size();
+  std::vector<Ref> ref(nv);
+  std::vector<bool> avail(nv, false);
+  // consumers of every var (statement indices), and whether it is an output
+  std::vector<std::vector<int>> users(nv);
+  for (size_t i = 0; i < f.body.size(); i++)
+    for (int v : stmt_inputs(f.body[i])) users[v].push_back((int)i);
+  std::vector<int> output_of(nv, -1);
+  for (size_t o = 0; o < f.output_vars.size(); o++) output_of[f.output_vars[o]] = (int)o;
+
+  for (int v = 0; v < nv; v++)
+    if (f.vars[v].param_index >= 0) {
+      ref[v] = Ref{Ref::Cur, f.vars[v].name, -1};
+      avail[v] = true;
+    }
+  // outputs that feed a state go to that state's second buffer
+  P.feedback.assign(f.output_vars.size(), "");
+  for (size_t o = 0; o < f.output_vars.size() && o < m->state.size(); o++) {
+    const int v = f.output_vars[o];
+    const std::string &st = m->state[o];
+    P.feedback[o] = st;
+    if (f.vars[v].dom != Dom::Spec)
+      throw tsm::CompileError{"'" + f.output_names[o] + "' is a grid field and cannot feed the "
+                              "spectral state '" + st + "'", -1, -1, f.name};
+    if (f.vars[v].param_index >= 0) {
+      if (f.vars[v].name != st)
+        throw tsm::CompileError{"output '" + f.output_names[o] + "' passes an argument through "
+                                "to state '" + st + "'; assign it instead", -1, -1, f.name};
+      continue;  // identity feedback: the state is unchanged
+    }
+    ref[v] = Ref{Ref::Next, st, -1};
+    P.swaps.insert(st);
+  }
+  // lazily evaluated views: v = synth(S) of a state input S that this
+  // program advances, read nowhere else
+  std::set<int> lazy;
+  if (is_step) {
+    for (size_t o = m->state.size(); o < f.output_vars.size(); o++) {
+      const int v = f.output_vars[o];
+      for (const auto &s : f.body)
+        if (s.kind == tsm::Stmt::Synth && s.out == v && f.vars[s.arg].param_index >= 0) {
+          const std::string &src = f.vars[s.arg].name;
+          bool is_state = std::find(m->state.begin(), m->state.end(), src) != m->state.end();
+          int other_users = 0;
+          for (int u : users[v]) (void)u, other_users++;
+          if (is_state && other_users == 0) {
+            lazy.insert(v);
+            P.lazy_views[f.output_names[o]] = src;
+          }
+        }
+    }
+  }
+  auto plan_buf = [&](int v) {
+    P.pcount.push_back(dom_count(f.vars[v].dom, p));
+    return Ref{Ref::Plan, "", (int)P.pcount.size() - 1};
+  };
+  auto materialize = [&](int v) {
+    if (ref[v].k == Ref::None) ref[v] = plan_buf(v);
+  };
+
+  std::vector<bool> done(f.body.size(), false);
+  auto all_done = [&]() { return std::all_of(done.begin(), done.end(), [](bool b) { return b; }); };
+  int tag = 0;
+  const std::string ptag = is_step ? "s" : "i";
+  while (!all_done()) {
+    bool progress = false;
+    // (A) spectral statements ready now
+    {
+      std::vector<int> grp;
+      std::set<int> local;
+      for (size_t i = 0; i < f.body.size(); i++) {
+        const auto &s = f.body[i];
+        if (done[i] || s.kind != tsm::Stmt::Elementwise || f.vars[s.out].dom != Dom::Spec) continue;
+        bool ok = true;
+        for (int v : stmt_inputs(s)) ok = ok && (avail[v] || local.count(v));
+        if (ok) {
+          grp.push_back((int)i);
+          local.insert(s.out);
+        }
+      }
+      if (!grp.empty()) {
+        Stage st;
+        st.kind = Stage::SpecEW;
+        std::set<int> ins;
+        for (int i : grp)
+          for (int v : stmt_inputs(f.body[i]))
+            if (!local.count(v)) ins.insert(v);
+        for (int v : ins) st.in.push_back(ref[v]);
+        std::set<int> grp_set(grp.begin(), grp.end());
+        std::vector<int> outs;
+        for (int i : grp) {
+          const int v = f.body[i].out;
+          bool needed = output_of[v] >= 0;
+          for (int u : users[v]) needed = needed || !grp_set.count(u);
+          if (needed) {
+            materialize(v);
+            outs.push_back(v);
+            st.out.push_back(ref[v]);
+          }
+          done[i] = true;
+        }
+        for (int v : outs) avail[v] = true;
+        // generated kernel
+        Emitter em{f, {}};
+        const std::string kn = "ts_specew_" + ptag + std::to_string(tag++);
+        std::ostringstream src;
+        src << "extern \"C\" __global__ void __launch_bounds__(256) " << kn
+            << "(TsSpecIO io) {\n"
+            << "  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+            << "  if (idx >= io.n) return;\n  const long inst = blockIdx.y;\n"
+            << "  const float *prm = io.prm + inst * io.nprm;\n"
+            << em.scalars();
+        int k = 0;
+        for (int v : ins) {
+          em.name[v] = "v" + std::to_string(v);
+          src << "  const float v" << v << " = io.sin[" << k << "][inst * io.sin_stride[" << k
+              << "] + idx];\n";
+          k++;
+        }
+        for (int i : grp) {
+          const auto &s = f.body[i];
+          src << "  const float v" << s.out << " = " << em.e(s.expr) << ";  // "
+              << f.vars[s.out].name << "\n";
+          em.name[s.out] = "v" + std::to_string(s.out);
+        }
+        for (size_t o = 0; o < outs.size(); o++)
+          src << "  io.sout[" << o << "][inst * io.sout_stride[" << o << "] + idx] = v" << outs[o]
+              << ";\n";
+        src << "}\n";
+        st.expr = kn;
+        st.label = "kernel  " + std::to_string(grp.size()) + " spectral statement(s)";
+        st.src = src.str();
+        P.stages.push_back(st);
+        progress = true;
+        continue;
+      }
+    }
+    // (B) a grid phase
+    std::vector<int> S, G, A;
+    std::set<int> local;
+    for (size_t i = 0; i < f.body.size(); i++) {
+      const auto &s = f.body[i];
+      if (!done[i] && s.kind == tsm::Stmt::Synth && avail[s.arg]) {
+        S.push_back((int)i);
+        local.insert(s.out);
+      }
+    }
+    for (size_t i = 0; i < f.body.size(); i++) {
+      const auto &s = f.body[i];
+      if (done[i] || s.kind != tsm::Stmt::Elementwise || f.vars[s.out].dom != Dom::Grid) continue;
+      bool ok = true;
+      for (int v : stmt_inputs(s)) ok = ok && (avail[v] || local.count(v));
+      if (ok) {
+        G.push_back((int)i);
+        local.insert(s.out);
+      }
+    }
+    for (size_t i = 0; i < f.body.size(); i++) {
+      const auto &s = f.body[i];
+      if (!done[i] && s.kind == tsm::Stmt::Analys && (avail[s.arg] || local.count(s.arg)))
+        A.push_back((int)i);
+    }
+    if (S.empty() && G.empty() && A.empty()) {
+      if (!progress)
+        throw tsm::CompileError{"internal: statements could not be scheduled", -1, -1, f.name};
+      continue;
+    }
+    std::set<int> phase(S.begin(), S.end());
+    phase.insert(G.begin(), G.end());
+    phase.insert(A.begin(), A.end());
+    // grid inputs already in buffers
+    std::set<int> gin;
+    for (int i : G)
+      for (int v : stmt_inputs(f.body[i]))
+        if (!local.count(v)) gin.insert(v);
+    for (int i : A)
+      if (!local.count(f.body[i].arg)) gin.insert(f.body[i].arg);
+    // grid values computed here that must reach memory
+    std::vector<int> gout;
+    for (int v : local) {
+      if (lazy.count(v)) continue;
+      bool needed = output_of[v] >= 0;
+      for (int u : users[v]) needed = needed || !phase.count(u);
+      if (needed) {
+        materialize(v);
+        gout.push_back(v);
+      }
+    }
+    if ((int)gin.size() > TS_MAXIO || (int)gout.size() > TS_MAXIO || (int)S.size() > TS_MAXIO)
+      throw tsm::CompileError{"too many grid fields in one phase (limit 8)", -1, -1, f.name};
+    if (!S.empty()) {
+      Stage st;
+      st.kind = Stage::LegSynth;
+      for (int i : S) st.in.push_back(ref[f.body[i].arg]);
+      st.nsyn = (int)S.size();
+      st.label = "legsyn  " + std::to_string(S.size()) + " field(s)";
+      P.stages.push_back(st);
+    }
+    {
+      Stage st;
+      st.kind = Stage::Phase;
+      st.nsyn = (int)S.size();
+      st.nana = (int)A.size();
+      for (int v : gin) st.in.push_back(ref[v]);
+      for (int v : gout) st.out.push_back(ref[v]);
+      Emitter em{f, {}};
+      const std::string pn = "TsProg_" + ptag + std::to_string(tag++);
+      std::ostringstream src;
+      src << "struct " << pn << " {\n  static constexpr int NSYN = " << S.size()
+          << ", NGIN = " << gin.size() << ", NANA = " << A.size() << ", NGOUT = " << gout.size()
+          << ";\n  static __device__ __forceinline__ void eval(const float *in, float *out, "
+             "const float *prm) {\n"
+          << em.scalars();
+      for (size_t k = 0; k < S.size(); k++) {
+        const int v = f.body[S[k]].out;
+        src << "    const float v" << v << " = in[" << k << "];  // " << f.vars[v].name << "\n";
+        em.name[v] = "v" + std::to_string(v);
+      }
+      int k = (int)S.size();
+      for (int v : gin) {
+        src << "    const float v" << v << " = in[" << k++ << "];  // " << f.vars[v].name << "\n";
+        em.name[v] = "v" + std::to_string(v);
+      }
+      for (int i : G) {
+        const auto &s = f.body[i];
+        src << "    const float v" << s.out << " = " << em.e(s.expr) << ";  // "
+            << f.vars[s.out].name << "\n";
+        em.name[s.out] = "v" + std::to_string(s.out);
+      }
+      for (size_t a = 0; a < A.size(); a++)
+        src << "    out[" << a << "] = " << em.name.at(f.body[A[a]].arg) << ";\n";
+      for (size_t o = 0; o < gout.size(); o++)
+        src << "    out[" << A.size() + o << "] = " << em.name.at(gout[o]) << ";\n";
+      src << "  }\n};\n";
+      st.expr = "ts_fourier_phase<" + pn + ">";
+      st.label = "phase   " + std::to_string(S.size()) + " synth, " + std::to_string(G.size()) +
+                 " grid statement(s), " + std::to_string(A.size()) + " analys";
+      st.src = src.str();
+      P.stages.push_back(st);
+      P.nsyn_max = std::max(P.nsyn_max, (int)S.size());
+      P.nana_max = std::max(P.nana_max, (int)A.size());
+    }
+    for (int i : phase) done[i] = true;
+    for (int v : gout) avail[v] = true;
+    if (A.empty()) continue;
+    // (C) analysis with the spectral statements that consume it as epilogue
+    std::set<int> aouts;
+    for (int i : A) aouts.insert(f.body[i].out);
+    std::vector<int> E;
+    std::set<int> elocal = aouts;
+    for (size_t i = 0; i < f.body.size(); i++) {
+      const auto &s = f.body[i];
+      if (done[i] || s.kind != tsm::Stmt::Elementwise || f.vars[s.out].dom != Dom::Spec) continue;
+      bool ok = true, uses_a = false;
+      for (int v : stmt_inputs(s)) {
+        ok = ok && (avail[v] || elocal.count(v));
+        uses_a = uses_a || elocal.count(v);
+      }
+      if (ok && uses_a) {
+        E.push_back((int)i);
+        elocal.insert(s.out);
+      }
+    }
+    std::set<int> eset(E.begin(), E.end());
+    std::set<int> sin;
+    for (int i : E)
+      for (int v : stmt_inputs(f.body[i]))
+        if (!elocal.count(v)) sin.insert(v);
+    std::vector<int> sout;
+    for (int v : elocal) {
+      bool needed = output_of[v] >= 0;
+      for (int u : users[v]) needed = needed || !eset.count(u);
+      if (needed) {
+        materialize(v);
+        sout.push_back(v);
+      }
+    }
+    if ((int)sin.size() > TS_MAXIO || (int)sout.size() > TS_MAXIO)
+      throw tsm::CompileError{"too many spectral fields in one epilogue (limit 8)", -1, -1, f.name};
+    Stage st;
+    st.kind = Stage::LegAnalys;
+    st.nana = (int)A.size();
+    for (int v : sin) st.in.push_back(ref[v]);
+    for (int v : sout) st.out.push_back(ref[v]);
+    ts_analys_shape(p, m->batch * st.nana, st.nana, &st.F, &st.K, &st.W, &st.per_cta);
+    Emitter em{f, {}};
+    const std::string en = "TsEpi_" + ptag + std::to_string(tag++);
+    std::ostringstream src;
+    src << "struct " << en << " {\n  TsSpecIO io;\n"
+        << "  __device__ __forceinline__ void operator()(long lm, int comp, const float *vals, "
+           "int f0, int nf, int F) const {\n"
+        << "    const long idx = 2 * lm + comp;\n"
+        << "    for (int i = 0; i < nf / " << A.size() << "; i++) {\n"
+        << "      const long inst = f0 / " << A.size() << " + i;\n"
+        << "      const float *prm = io.prm + inst * io.nprm;\n";
+    {
+      std::istringstream sc(em.scalars());
+      std::string line;
+      while (std::getline(sc, line)) src << "    " << line << "\n";
+    }
+    for (size_t a = 0; a < A.size(); a++) {
+      const int v = f.body[A[a]].out;
+      src << "      const float v" << v << " = vals[i * " << A.size() << " + " << a << "];  // "
+          << f.vars[v].name << "\n";
+      em.name[v] = "v" + std::to_string(v);
+    }
+    int k = 0;
+    for (int v : sin) {
+      src << "      const float v" << v << " = io.sin[" << k << "][inst * io.sin_stride[" << k
+          << "] + idx];  // " << f.vars[v].name << "\n";
+      em.name[v] = "v" + std::to_string(v);
+      k++;
+    }
+    for (int i : E) {
+      const auto &s = f.body[i];
+      src << "      const float v" << s.out << " = " << em.e(s.expr) << ";  // "
+          << f.vars[s.out].name << "\n";
+      em.name[s.out] = "v" + std::to_string(s.out);
+    }
+    for (size_t o = 0; o < sout.size(); o++)
+      src << "      io.sout[" << o << "][inst * io.sout_stride[" << o << "] + idx] = v"
+          << sout[o] << ";\n";
+    src << "    }\n  }\n};\n";
+    st.expr = "ts_leg_analys_f32<" + std::to_string(st.F) + ", " + std::to_string(st.K) + ", 2, " +
+              en + ">";
+    st.label = "legana  " + std::to_string(A.size()) + " field(s), " + std::to_string(E.size()) +
+               " spectral statement(s) fused";
+    st.src = src.str();
+    P.stages.push_back(st);
+    for (int i : E) done[i] = true;
+    for (int v : sout) avail[v] = true;
+  }
+  for (int o = 0; o < (int)f.output_vars.size(); o++) {
+    const int v = f.output_vars[o];
+    if (lazy.count(v)) continue;
+    if (ref[v].k == Ref::None) materialize(v);
+    P.value_ref[f.output_names[o]] = ref[v];
+  }
+  // every named (non-temporary) value that reached memory is readable
+  for (int v = 0; v < nv; v++)
+    if (!f.vars[v].temp && ref[v].k != Ref::None && !P.value_ref.count(f.vars[v].name))
+      P.value_ref[f.vars[v].name] = ref[v];
+  // reads happen after the run, when each state's second buffer has been
+  // swapped in: a value written to `next` is then in `cur`
+  for (auto &kv : P.value_ref)
+    if (kv.second.k == Ref::Next) kv.second.k = Ref::Cur;
+}
+
+std::string stage_source(const Stage &s) { return s.src; }
+std::string stage_title(const Stage &s) { return s.label; }
+
+// --------------------------------------------------------------------- NVRTC
+
+// NVRTC: the generated stages plus the kernel headers -> an sm_100a cubin,
+// and the lowered name of every template instantiation.
+std::vector<char> build_cubin(ts_model m, std::map<std::string, std::string> &lowered) {
+  std::ostringstream src;
+  src << "#include \"ts_common.cuh\"\n#include \"fourier.cuh\"\n#include \"leg_f32.cuh\"\n";
+  for (auto &P : m->prog)
+    for (auto &s : P.stages) src << stage_source(s);
+  const std::string code = src.str();
+  nvrtcProgram prog;
+  auto nv = [&](nvrtcResult r, const char *what) {
+    if (r != NVRTC_SUCCESS)
+      ts_throw(TS_ERR_COMPILE, std::string(what) + ": " + nvrtcGetErrorString(r));
+  };
+  nv(nvrtcCreateProgram(&prog, code.c_str(), "model.cu", ts_src_count, ts_src_texts, ts_src_names),
+     "nvrtcCreateProgram");
+  std::vector<std::string> exprs;
+  for (auto &P : m->prog)
+    for (auto &s : P.stages)
+      if (!s.expr.empty() && s.expr.find('<') != std::string::npos) {
+        exprs.push_back(s.expr);
+        nv(nvrtcAddNameExpression(prog, s.expr.c_str()), "nvrtcAddNameExpression");
+      }
+  const char *opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-lineinfo",
+                        "--device-as-default-execution-space"};
+  const nvrtcResult rc = nvrtcCompileProgram(prog, 4, opts);
+  if (rc != NVRTC_SUCCESS) {
+    size_t n = 0;
+    nvrtcGetProgramLogSize(prog, &n);
+    std::string log(n, '\0');
+    nvrtcGetProgramLog(prog, &log[0]);
+    nvrtcDestroyProgram(&prog);
+    ts_throw(TS_ERR_COMPILE, "generated CUDA failed to compile:\n" + log + "\n--- source ---\n" + code);
+  }
+  size_t n = 0;
+  nv(nvrtcGetCUBINSize(prog, &n), "nvrtcGetCUBINSize");
+  std::vector<char> cubin(n);
+  nv(nvrtcGetCUBIN(prog, cubin.data()), "nvrtcGetCUBIN");
+  for (auto &e : exprs) {
+    const char *ln = nullptr;
+    nv(nvrtcGetLoweredName(prog, e.c_str(), &ln), "nvrtcGetLoweredName");
+    lowered[e] = ln;
+  }
+  nvrtcDestroyProgram(&prog);
+  return cubin;
+}
+
+void compile_kernels(ts_model m) {
+  std::map<std::string, std::string> lowered;
+  const std::vector<char> cubin = build_cubin(m, lowered);
+  TS_CUDA(cudaLibraryLoadData(&m->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+  for (auto &P : m->prog)
+    for (auto &s : P.stages) {
+      if (s.expr.empty()) continue;
+      const std::string name = lowered.count(s.expr) ? lowered[s.expr] : s.expr;
+      TS_CUDA(cudaLibraryGetKernel(&s.kern, m->lib, name.c_str()));
+      if (s.smem > 48 * 1024)
+        TS_CUDA(cudaKernelSetAttributeForDevice(
+            s.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem, m->ctx->device));
+    }
+}
+
+// ------------------------------------------------------------------- runtime
+
+float *resolve(ts_model m, Program &P, const Ref &r, long *stride) {
+  if (r.k == Ref::Plan) {
+    *stride = P.pcount[r.pbuf];
+    return P.pbuf[r.pbuf];
+  }
+  HostBuf &h = m->host.at(r.host);
+  *stride = h.shared ? 0 : h.count;
+  return r.k == Ref::Next ? h.next : h.cur;
+}
+
+void fill_spec_io(ts_model m, Program &P, const Stage &s, TsSpecIO &io) {
+  memset(&io, 0, sizeof io);
+  for (size_t i = 0; i < s.in.size(); i++) io.sin[i] = resolve(m, P, s.in[i], &io.sin_stride[i]);
+  for (size_t i = 0; i < s.out.size(); i++) io.sout[i] = resolve(m, P, s.out[i], &io.sout_stride[i]);
+  io.prm = m->d_prm;
+  io.nprm = (int)m->params.size();
+  io.n = 2 * m->plan->nlm;
+}
+
+void run_program(ts_model m, Program &P, cudaStream_t st) {
+  ts_plan p = m->plan;
+  const long field = (long)(p->mmax + 1) * p->nlat;
+  float2 *fm = (float2 *)m->fm.p, *gm = (float2 *)m->gm.p;
+  const int B = m->batch;
+  for (auto &s : P.stages) {
+    switch (s.kind) {
+      case Stage::LegSynth: {
+        TsFields q{};
+        for (size_t i = 0; i < s.in.size(); i++) {
+          long stride;
+          q.base[i] = (const float2 *)resolve(m, P, s.in[i], &stride);
+          q.inst_stride[i] = stride / 2;
+        }
+        q.nper = s.nsyn;
+        ts_launch_leg_synth_fields(p, q, fm, field, B * s.nsyn, st);
+        break;
+      }
+      case Stage::Phase: {
+        TsPhaseIO io;
+        memset(&io, 0, sizeof io);
+        io.fm = fm;
+        io.gm = gm;
+        io.field = field;
+        for (size_t i = 0; i < s.in.size(); i++) io.gin[i] = resolve(m, P, s.in[i], &io.gin_stride[i]);
+        for (size_t i = 0; i < s.out.size(); i++)
+          io.gout[i] = resolve(m, P, s.out[i], &io.gout_stride[i]);
+        io.prm = m->d_prm;
+        io.nprm = (int)m->params.size();
+        TsFftTab ft = p->fft;
+        void *args[] = {&ft, &io};
+        dim3 grid((p->nlat + s.lb - 1) / s.lb, B);
+        TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(32 * s.lb), args, s.smem, st));
+        break;
+      }
+      case Stage::LegAnalys: {
+        // the epilogue functor is a TsSpecIO (first and only member)
+        TsSpecIO epi;
+        fill_spec_io(m, P, s, epi);
+        TsLegTab leg = p->leg;
+        const float2 *g = gm;
+        long gs = field;
+        int nfields = B * s.nana;
+        int per_cta = s.per_cta;
+        void *args[] = {&leg, &g, &gs, &epi, &nfields, &per_cta};
+        dim3 grid(p->mmax + 1, (nfields + per_cta - 1) / per_cta);
+        TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(32 * s.W), args, s.smem, st));
+        break;
+      }
+      case Stage::SpecEW: {
+        TsSpecIO io;
+        fill_spec_io(m, P, s, io);
+        void *args[] = {&io};
+        dim3 grid((unsigned)((2 * p->nlm + 255) / 256), B);
+        TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(256), args, 0, st));
+        break;
+      }
+    }
+  }
+  for (auto &name : P.swaps) {
+    HostBuf &h = m->host.at(name);
+    std::swap(h.cur, h.next);
+  }
+}
+
+void finish_shapes(ts_model m) {
+  ts_plan p = m->plan;
+  for (auto &P : m->prog)
+    for (auto &s : P.stages) {
+      if (s.kind == Stage::Phase) {
+        const int nrows = s.nsyn + s.nana + 1;
+        s.lb = ts_fourier_lb(p, m->batch, nrows, &s.smem);
+      } else if (s.kind == Stage::LegAnalys) {
+        s.smem = ts_analys_smem(p, s.F, s.W);
+      }
+    }
+}
+
+void free_model(ts_model m) {
+  for (auto &kv : m->host) {
+    if (kv.second.cur) cudaFree(kv.second.cur);
+    if (kv.second.next) cudaFree(kv.second.next);
+  }
+  for (auto &P : m->prog)
+    for (float *b : P.pbuf)
+      if (b) cudaFree(b);
+  if (m->d_prm) cudaFree(m->d_prm);
+  m->fm.release();
+  m->gm.release();
+  m->stash.release();
+  if (m->lib) cudaLibraryUnload(m->lib);
+}
+
+float *dalloc(long n) {
+  float *p = nullptr;
+  TS_CUDA(cudaMalloc(&p, sizeof(float) * std::max<long>(n, 1)));
+  TS_CUDA(cudaMemset(p, 0, sizeof(float) * std::max<long>(n, 1)));
+  return p;
+}
+
+void check_finite_params(std::vector<float> &v) {
+  for (float &x : v)
+    if (!std::isfinite(x)) x = 0.0f;  // plan.ts:414-416: non-finite values become 0
+}
+
+// Laplace-Beltrami eigenvalues l(l+1), duplicated over re/im (model.ts:46-56)
+std::vector<float> eigenvalues(ts_plan p) {
+  std::vector<float> lam(2 * p->nlm);
+  for (int mm = 0; mm <= p->mmax; mm++)
+    for (int l = mm; l <= p->lmax; l++) {
+      const long i = ts_lm_index(p->lmax, l, mm);
+      lam[2 * i] = lam[2 * i + 1] = (float)l * (l + 1);
+    }
+  return lam;
+}
+
+// which program's buffer holds `name` now (GpuModel.#locate, model.ts:243-252)
+bool locate(ts_model m, const std::string &name, float **ptr, long *count, long *stride,
+            std::string *lazy_state) {
+  const int first = m->last_ran, second = 1 - m->last_ran;
+  for (int which : {first, second}) {
+    Program &P = m->prog[which];
+    auto lz = P.lazy_views.find(name);
+    if (lz != P.lazy_views.end()) {
+      *lazy_state = lz->second;
+      *ptr = nullptr;
+      *count = (long)m->plan->nlat * m->plan->nphi;
+      *stride = *count;
+      return true;
+    }
+    auto it = P.value_ref.find(name);
+    if (it != P.value_ref.end()) {
+      *ptr = resolve(m, P, it->second, stride);
+      *count = it->second.k == Ref::Plan ? P.pcount[it->second.pbuf]
+                                          : m->host.at(it->second.host).count;
+      lazy_state->clear();
+      return true;
+    }
+  }
+  auto h = m->host.find(name);
+  if (h != m->host.end()) {
+    *ptr = h->second.cur;
+    *count = h->second.count;
+    *stride = h->second.shared ? 0 : h->second.count;
+    lazy_state->clear();
+    return true;
+  }
+  return false;
+}
+
+// parse, specialise init/step and schedule them; fills `err` on rejection
+void front_end(ts_model m, int nstate, int nview, ts_compile_error *err) {
+  ts_plan plan = m->plan;
+  const long npts = (long)plan->nlat * plan->nphi, nlm = plan->nlm;
+  // the bindings a .m may name (model.ts:116-125)
+  std::map<std::string, tsm::Binding> b;
+  b["lam"] = {tsm::Binding::Tensor, Dom::Spec, 0};
+  b["noise"] = {tsm::Binding::Tensor, Dom::Grid, 0};
+  b["npts"] = {tsm::Binding::Const, Dom::Scalar, (double)npts};
+  b["nlm"] = {tsm::Binding::Const, Dom::Scalar, (double)nlm};
+  for (auto &s : m->state) b[s] = {tsm::Binding::Tensor, Dom::Spec, 0};
+  for (auto &s : m->params) b[s] = {tsm::Binding::Param, Dom::Scalar, 0};
+  const tsm::Grid g{npts, nlm};
+  try {
+    const auto file = tsm::parse_model(m->source);
+    const int nargout = nstate + nview;
+    m->prog[0].fn = tsm::specialize(file, "init", b, m->params, nargout, g);
+    m->prog[1].fn = tsm::specialize(file, "step", b, m->params, nargout, g);
+    schedule(m, m->prog[0], false);
+    schedule(m, m->prog[1], true);
+  } catch (const tsm::CompileError &ce) {
+    if (err) {
+      err->start = ce.start;
+      err->end = ce.end;
+      snprintf(err->fn, sizeof err->fn, "%s", ce.fn.c_str());
+      snprintf(err->message, sizeof err->message, "%s", ce.message.c_str());
+    }
+    ts_throw(TS_ERR_COMPILE, ce.message);
+  }
+}
+
+std::string describe_program(const Program &P) {
+  std::string s = tsm::describe(P.fn);
+  for (size_t o = 0; o < P.feedback.size(); o++)
+    if (!P.feedback[o].empty()) s += "copy    " + P.fn.output_names[o] + " -> " + P.feedback[o] + "\n";
+  s += "-- launches --\n";
+  for (const auto &st : P.stages) s += stage_title(st) + "\n";
+  return s;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+
+extern "C" {
+
+int ts_model_compile(ts_plan plan, const char *source, const char *const *state, int nstate,
+                     const char *const *view, int nview, const char *const *params, int nparams,
+                     int batch, ts_model *out, ts_compile_error *err) {
+  ts_ctx ctx = plan ? plan->ctx : nullptr;
+  ts_model m = nullptr;
+  if (err) memset(err, 0, sizeof(*err));
+  try {
+    TS_REQUIRE(plan && source && out, TS_ERR_INVALID, "null argument");
+    TS_REQUIRE(nstate >= 1 && nstate <= TS_MAXIO && nview >= 0 && nparams >= 0, TS_ERR_INVALID,
+               "bad state/view/param counts");
+    TS_REQUIRE(batch >= 1 && batch <= 65535, TS_ERR_INVALID, "batch must be in [1, 65535]");
+    TS_REQUIRE(plan->fourier == TS_FOURIER_FFT, TS_ERR_UNSUPPORTED,
+               "models need an FFT grid: nphi = 2^a 3^b (the fused phase kernel runs the FFT)");
+    TS_CUDA(cudaSetDevice(ctx->device));
+    m = new ts_model_s();
+    m->ctx = ctx;
+    m->plan = plan;
+    m->batch = batch;
+    m->source = source;
+    for (int i = 0; i < nstate; i++) m->state.push_back(state[i]);
+    for (int i = 0; i < nview; i++) m->view.push_back(view[i]);
+    for (int i = 0; i < nparams; i++) m->params.push_back(params[i]);
+    front_end(m, nstate, nview, err);
+    finish_shapes(m);
+    compile_kernels(m);
+    const long npts = (long)plan->nlat * plan->nphi, nlm = plan->nlm;
+        // host-owned buffers: state (two each), eigenvalues (shared), noise
+    for (auto &s : m->state) {
+      HostBuf h{Dom::Spec, 2 * nlm, false, true, dalloc(2 * nlm * batch), dalloc(2 * nlm * batch)};
+      m->host[s] = h;
+    }
+    m->host["lam"] = HostBuf{Dom::Spec, 2 * nlm, true, false, dalloc(2 * nlm), nullptr};
+    m->host["noise"] = HostBuf{Dom::Grid, npts, false, false, dalloc(npts * batch), nullptr};
+    const auto lam = eigenvalues(plan);
+    TS_CUDA(cudaMemcpy(m->host["lam"].cur, lam.data(), sizeof(float) * lam.size(),
+                       cudaMemcpyHostToDevice));
+    for (auto &P : m->prog)
+      for (long c : P.pcount) P.pbuf.push_back(dalloc(c * batch));
+    const long field = (long)(plan->mmax + 1) * plan->nlat;
+    const int nsyn = std::max({m->prog[0].nsyn_max, m->prog[1].nsyn_max, 1});
+    const int nana = std::max({m->prog[0].nana_max, m->prog[1].nana_max, 1});
+    m->fm.ensure(sizeof(float2) * field * nsyn * batch);
+    m->gm.ensure(sizeof(float2) * field * nana * batch);
+    m->stash.ensure(sizeof(float) * 2 * nlm * batch * nstate);
+    m->h_prm.assign((size_t)std::max(nparams, 1) * batch, 0.0f);
+    m->d_prm = dalloc((long)m->h_prm.size());
+    *out = m;
+    return TS_OK;
+  } catch (const ts_exc &e) {
+    if (err && err->message[0] == 0) snprintf(err->message, sizeof err->message, "%s", e.msg.c_str());
+    if (m) {
+      free_model(m);
+      delete m;
+    }
+    ts_set_error(ctx, e.msg);
+    return e.code;
+  }
+}
+
+int ts_model_destroy(ts_model m) {
+  if (!m) return TS_ERR_INVALID;
+  cudaSetDevice(m->ctx->device);
+  cudaStreamSynchronize(m->ctx->stream);
+  free_model(m);
+  delete m;
+  return TS_OK;
+}
+
+#define TSM_BEGIN(m)                                   \
+  ts_ctx ctx = m ? m->ctx : nullptr;                   \
+  try {                                                \
+    TS_REQUIRE(m != nullptr, TS_ERR_INVALID, "null model"); \
+    TS_CUDA(cudaSetDevice(ctx->device));
+#define TSM_END                                         \
+  }                                                     \
+  catch (const ts_exc &e) {                             \
+    ts_set_error(ctx, e.msg);                           \
+    return e.code;                                      \
+  }                                                     \
+  return TS_OK;
+
+int ts_model_set_params(ts_model m, const float *values, int n) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(n == (int)m->params.size(), TS_ERR_SIZE, "set_params: expected one value per parameter");
+  const int np = std::max(n, 1);
+  for (int i = 0; i < m->batch; i++)
+    for (int k = 0; k < n; k++) m->h_prm[(size_t)i * np + k] = values[k];
+  check_finite_params(m->h_prm);
+  TS_CUDA(cudaMemcpyAsync(m->d_prm, m->h_prm.data(), sizeof(float) * m->h_prm.size(),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  TS_CUDA(cudaStreamSynchronize(ctx->stream));
+  TSM_END
+}
+
+int ts_model_set_params_batched(ts_model m, const float *values, int batch, int n) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(n == (int)m->params.size() && batch == m->batch, TS_ERR_SIZE,
+             "set_params_batched: expected batch x nparams values");
+  if (n > 0) std::copy(values, values + (size_t)batch * n, m->h_prm.begin());
+  check_finite_params(m->h_prm);
+  TS_CUDA(cudaMemcpyAsync(m->d_prm, m->h_prm.data(), sizeof(float) * m->h_prm.size(),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  TS_CUDA(cudaStreamSynchronize(ctx->stream));
+  TSM_END
+}
+
+int ts_model_upload(ts_model m, const char *name, const float *data, long n) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(name && data, TS_ERR_INVALID, "null argument");
+  auto it = m->host.find(name);
+  if (it == m->host.end()) ts_throw(TS_ERR_NOT_FOUND, std::string("upload: no buffer named '") + name + "'");
+  HostBuf &h = it->second;
+  const long total = h.shared ? h.count : h.count * m->batch;
+  if (n != h.count && n != total) {
+    char buf[200];
+    snprintf(buf, sizeof buf, "upload '%s': expected %ld elements, got %ld", name, total, n);
+    ts_throw(TS_ERR_SIZE, buf);
+  }
+  if (n == total) {
+    TS_CUDA(cudaMemcpyAsync(h.cur, data, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  } else {  // one instance's worth: the same values for every instance
+    for (int i = 0; i < m->batch; i++)
+      TS_CUDA(cudaMemcpyAsync(h.cur + (long)i * h.count, data, sizeof(float) * n,
+                              cudaMemcpyHostToDevice, ctx->stream));
+  }
+  TS_CUDA(cudaStreamSynchronize(ctx->stream));
+  TSM_END
+}
+
+int ts_model_init(ts_model m, const float *noise, long n) {
+  TSM_BEGIN(m)
+  if (noise) {
+    const int rc = ts_model_upload(m, "noise", noise, n);
+    if (rc != TS_OK) return rc;
+  }
+  run_program(m, m->prog[0], ctx->stream);
+  m->last_ran = 0;
+  TSM_END
+}
+
+int ts_model_step(ts_model m, int nsteps) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(nsteps >= 0, TS_ERR_INVALID, "nsteps must be >= 0");
+  for (int i = 0; i < nsteps; i++) run_program(m, m->prog[1], ctx->stream);
+  if (nsteps > 0) m->last_ran = 1;
+  TSM_END
+}
+
+int ts_model_read(ts_model m, const char *name, float *out, long n) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(name && out, TS_ERR_INVALID, "null argument");
+  float *ptr;
+  long count, stride;
+  std::string lazy;
+  if (!locate(m, name, &ptr, &count, &stride, &lazy))
+    ts_throw(TS_ERR_NOT_FOUND, std::string("read: the model has no value named '") + name + "'");
+  const long total = count * m->batch;
+  TS_REQUIRE(n == total || n == count, TS_ERR_SIZE,
+             std::string("read '") + name + "': expected " + std::to_string(total) + " (or " +
+                 std::to_string(count) + " for instance 0) elements");
+  const int ninst = n == total ? m->batch : 1;
+  ts_plan p = m->plan;
+  if (!lazy.empty()) {
+    // a displayed field computed on demand from the state it is synth() of
+    HostBuf &h = m->host.at(lazy);
+    const float *src = m->prog[1].swaps.count(lazy) ? h.next : h.cur;
+    const long field = (long)(p->mmax + 1) * p->nlat;
+    p->fm.ensure(sizeof(float2) * field * ninst);
+    ts_launch_leg_synth(p, (const float2 *)src, p->nlm, (float2 *)p->fm.p, field, ninst, ctx->stream);
+    float *tmp = nullptr;
+    TS_CUDA(cudaMallocAsync(&tmp, sizeof(float) * count * ninst, ctx->stream));
+    ts_launch_fourier_synth(p, (const float2 *)p->fm.p, field, tmp, count, ninst, ctx->stream);
+    TS_CUDA(cudaMemcpyAsync(out, tmp, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    TS_CUDA(cudaFreeAsync(tmp, ctx->stream));
+  } else if (stride == 0 && ninst > 1) {
+    for (int i = 0; i < ninst; i++)
+      TS_CUDA(cudaMemcpyAsync(out + (long)i * count, ptr, sizeof(float) * count,
+                              cudaMemcpyDeviceToHost, ctx->stream));
+  } else {
+    TS_CUDA(cudaMemcpyAsync(out, ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  TS_CUDA(cudaStreamSynchronize(ctx->stream));
+  TSM_END
+}
+
+int ts_model_value_ptr(ts_model m, const char *name, float **dev, long *count) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(name && dev && count, TS_ERR_INVALID, "null argument");
+  float *ptr;
+  long stride;
+  std::string lazy;
+  if (!locate(m, name, &ptr, count, &stride, &lazy) || !lazy.empty())
+    ts_throw(TS_ERR_NOT_FOUND, std::string("no device buffer holds '") + name + "'");
+  *dev = ptr;
+  TSM_END
+}
+
+int ts_model_snapshot(ts_model m) {
+  TSM_BEGIN(m)
+  const long n = 2 * m->plan->nlm * m->batch;
+  long off = 0;
+  for (auto &s : m->state) {
+    TS_CUDA(cudaMemcpyAsync((float *)m->stash.p + off, m->host.at(s).cur, sizeof(float) * n,
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+    off += n;
+  }
+  m->stashed_ran = m->last_ran;
+  TSM_END
+}
+
+int ts_model_restore(ts_model m) {
+  TSM_BEGIN(m)
+  const long n = 2 * m->plan->nlm * m->batch;
+  long off = 0;
+  for (auto &s : m->state) {
+    TS_CUDA(cudaMemcpyAsync(m->host.at(s).cur, (float *)m->stash.p + off, sizeof(float) * n,
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+    off += n;
+  }
+  m->last_ran = m->stashed_ran;
+  TSM_END
+}
+
+int ts_model_describe(ts_model m, int which, char *buf, size_t cap) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(which == 0 || which == 1, TS_ERR_INVALID, "which: 0 = init, 1 = step");
+  TS_REQUIRE(buf && cap > 0, TS_ERR_INVALID, "null buffer");
+  snprintf(buf, cap, "%s", describe_program(m->prog[which]).c_str());
+  TSM_END
+}
+
+int ts_model_source(ts_model m, char *buf, size_t cap) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(buf && cap > 0, TS_ERR_INVALID, "null buffer");
+  std::string s;
+  for (auto &P : m->prog)
+    for (auto &st : P.stages) s += stage_source(st);
+  snprintf(buf, cap, "%s", s.c_str());
+  TSM_END
+}
+
+int ts_model_counts(ts_model m, int which, int *kernels, int *launches) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(which == 0 || which == 1, TS_ERR_INVALID, "which: 0 = init, 1 = step");
+  if (kernels) *kernels = tsm::count_kernels(m->prog[which].fn);
+  if (launches) *launches = (int)m->prog[which].stages.size();
+  TSM_END
+}
+
+// Everything ts_model_compile does short of the GPU: parse, specialise,
+// schedule, generate CUDA and compile it with NVRTC for sm_100a, on a grid
+// described by its sizes.  Writes describe() of init and step (separated by a
+// line "====") to `describe` and the kernel and launch counts of step.
+int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
+                   const char *const *state, int nstate, const char *const *view, int nview,
+                   const char *const *params, int nparams, int batch, char *describe,
+                   size_t cap, int *kernels, int *launches, ts_compile_error *err) {
+  if (err) memset(err, 0, sizeof(*err));
+  ts_ctx_s ctx;
+  ctx.sm_count = 148;
+  ctx.smem_optin = 232448;
+  ts_plan_s plan;
+  ts_model_s mod;
+  try {
+    TS_REQUIRE(source != nullptr, TS_ERR_INVALID, "null source");
+    char why[256];
+    if (ts_validate_config(lmax, mmax, nlat, nphi, why, sizeof why) != TS_OK)
+      ts_throw(TS_ERR_INVALID, why);
+    plan.ctx = &ctx;
+    plan.lmax = lmax;
+    plan.mmax = mmax;
+    plan.nlat = nlat;
+    plan.nphi = nphi;
+    plan.nh = (nlat + 1) / 2;
+    plan.nlm = ts_nlm_calc(lmax, mmax);
+    plan.fft.nphi = nphi;
+    plan.fft.H = nphi / 2;
+    plan.fft.mmax = mmax;
+    plan.fft.nlat = nlat;
+    mod.ctx = &ctx;
+    mod.plan = &plan;
+    mod.batch = batch;
+    mod.source = source;
+    for (int i = 0; i < nstate; i++) mod.state.push_back(state[i]);
+    for (int i = 0; i < nview; i++) mod.view.push_back(view[i]);
+    for (int i = 0; i < nparams; i++) mod.params.push_back(params[i]);
+    front_end(&mod, nstate, nview, err);
+    finish_shapes(&mod);
+    std::map<std::string, std::string> lowered;
+    build_cubin(&mod, lowered);
+    if (describe && cap)
+      snprintf(describe, cap, "%s====\n%s", describe_program(mod.prog[0]).c_str(),
+               describe_program(mod.prog[1]).c_str());
+    if (kernels) *kernels = tsm::count_kernels(mod.prog[1].fn);
+    if (launches) *launches = (int)mod.prog[1].stages.size();
+    return TS_OK;
+  } catch (const ts_exc &e) {
+    if (err && err->message[0] == 0) snprintf(err->message, sizeof err->message, "%s", e.msg.c_str());
+    ts_set_error(nullptr, e.msg);
+    return e.code;
+  }
+}
+
+}  // extern "C"

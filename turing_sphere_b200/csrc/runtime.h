@@ -91,5 +91,13 @@ void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fm_stride, float 
                              long spat_stride, int nfields, cudaStream_t s);
 void ts_launch_fourier_analys(ts_plan p, const float *spat, long spat_stride, float2 *g,
                               long g_stride, int nfields, cudaStream_t s);
+void ts_launch_leg_synth_fields(ts_plan p, const TsFields &q, float2 *fm, long fm_stride,
+                                int nfields, cudaStream_t s);
+// analysis launch shape: fields per CTA F (template), latitudes per thread K,
+// warps W; groups = fields handled per CTA (a multiple of `per_inst`)
+void ts_analys_shape(ts_plan p, int nfields, int per_inst, int *F, int *K, int *W, int *per_cta);
+size_t ts_analys_smem(ts_plan p, int F, int W);
+// rows per Fourier CTA for a kernel holding `nrows` rows per warp
+int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem);
 void ts_init_tables(ts_plan p);
 void ts_kernel_attrs_once(ts_ctx ctx);

@@ -1,6 +1,7 @@
 // Plan tables (FP64 on the GPU) and launchers of the plain FP32 transform
 // kernels.
 #include <cmath>
+#include <type_traits>
 
 #include "kernels/fourier.cuh"
 #include "kernels/leg_f32.cuh"
@@ -199,7 +200,11 @@ void leg_synth_t(ts_plan p, const float2 *q, long qs, float2 *fm, long fs, int n
   const int bd = p->nh >= 128 ? 64 : 32;
   dim3 grid((p->nh + bd - 1) / bd, p->mmax + 1, (nf + F - 1) / F);
   const size_t smem = sizeof(float2) * (size_t)(p->lmax + 1) * (1 + F);
-  ts_leg_synth_f32<F><<<grid, bd, smem, s>>>(p->leg, q, qs, fm, fs, nf);
+  TsFields qf{};
+  qf.base[0] = q;
+  qf.inst_stride[0] = qs;
+  qf.nper = 1;
+  ts_leg_synth_f32<F><<<grid, bd, smem, s>>>(p->leg, qf, fm, fs, nf);
   TS_CUDA(cudaGetLastError());
 }
 
@@ -211,7 +216,7 @@ void leg_analys_t(ts_plan p, int W, const float2 *g, long gs, float2 *q, long qs
   dim3 grid(p->mmax + 1, (nf + F - 1) / F);
   const size_t smem = sizeof(float2) * (p->lmax + 1) + sizeof(float) * (size_t)(W * N + N);
   TsAnalysStore epi{q, qs};
-  ts_leg_analys_f32<F, K, P, TsAnalysStore><<<grid, 32 * W, smem, s>>>(p->leg, g, gs, epi, nf);
+  ts_leg_analys_f32<F, K, P, TsAnalysStore><<<grid, 32 * W, smem, s>>>(p->leg, g, gs, epi, nf, F);
   TS_CUDA(cudaGetLastError());
 }
 
@@ -228,24 +233,34 @@ void leg_analys_f(ts_plan p, int K, int W, const float2 *g, long gs, float2 *q, 
   }
 }
 
-// latitudes per thread (K) and warps (W) for the analysis: cover nh with the
-// least idle lanes, preferring more warps.
+// latitudes per thread (K) and warps (W) for the analysis.  The warp
+// reduction costs about 2 operations per reduced value against K*4 useful
+// FMAs, so K is taken as large as possible (up to 8) with the least idle
+// lanes; more CTAs, not more warps per CTA, supply the parallelism.
 void pick_kw(int nh, int &K, int &W) {
-  static const int Ks[] = {1, 2, 3, 4, 6, 8};
+  static const int Ks[] = {8, 6, 4, 3, 2, 1};
   int best = 1 << 30;
   K = 8;
   W = 8;
-  for (int w = 8; w >= 1; w--)
-    for (int k : Ks) {
+  for (int k : Ks)
+    for (int w = 1; w <= 8; w++) {
       const int cap = 32 * w * k;
       if (cap < nh) continue;
       const int waste = cap - nh;
-      if (waste < best) {
-        best = waste;
-        K = k;
-        W = w;
+      // prefer less waste; accept up to 1/8 idle lanes for a larger K
+      if (waste * 8 <= cap && waste < best + 32 * k / 4) {
+        if (best == (1 << 30) || waste < best) {
+          best = waste;
+          K = k;
+          W = w;
+        }
       }
+      break;
     }
+  if (best == (1 << 30)) {  // tiny grids: one warp, one latitude per lane
+    K = 1;
+    W = (nh + 31) / 32;
+  }
 }
 
 // rows (warps) per Fourier CTA: as many as shared memory allows, fewer when
@@ -280,6 +295,46 @@ void ts_kernel_attrs_once(ts_ctx ctx) {
   done = true;
 }
 
+void ts_launch_leg_synth_fields(ts_plan p, const TsFields &q, float2 *fm, long fs, int nf,
+                                cudaStream_t s) {
+  const int bd = p->nh >= 128 ? 64 : 32;
+  auto go = [&](auto Fc) {
+    constexpr int F = decltype(Fc)::value;
+    dim3 grid((p->nh + bd - 1) / bd, p->mmax + 1, (nf + F - 1) / F);
+    const size_t smem = sizeof(float2) * (size_t)(p->lmax + 1) * (1 + F);
+    ts_leg_synth_f32<F><<<grid, bd, smem, s>>>(p->leg, q, fm, fs, nf);
+    TS_CUDA(cudaGetLastError());
+  };
+  if (nf >= 8) return go(std::integral_constant<int, 8>());
+  if (nf >= 4) return go(std::integral_constant<int, 4>());
+  if (nf >= 2) return go(std::integral_constant<int, 2>());
+  return go(std::integral_constant<int, 1>());
+}
+
+void ts_analys_shape(ts_plan p, int nfields, int per_inst, int *F, int *K, int *W, int *per_cta) {
+  pick_kw(p->nh, *K, *W);
+  int f = 4;
+  while (f > 1 && *K * f > 24) f >>= 1;
+  while (f < per_inst) f <<= 1;  // a CTA holds at least one whole instance
+  int groups = f / per_inst;
+  if (nfields < f) {
+    f = 1;
+    while (f < nfields) f <<= 1;
+    groups = (f / per_inst) > 0 ? f / per_inst : 1;
+  }
+  *F = f;
+  *per_cta = groups * per_inst;
+}
+
+size_t ts_analys_smem(ts_plan p, int F, int W) {
+  const int N = 4 * 2 * F;
+  return sizeof(float2) * (p->lmax + 1) + sizeof(float) * (size_t)(W * N + N);
+}
+
+int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem) {
+  return pick_lb(p, nblocks_y, nrows, smem);
+}
+
 void ts_launch_leg_synth(ts_plan p, const float2 *q, long qs, float2 *fm, long fs, int nf,
                          cudaStream_t s) {
   if (nf >= 8) return leg_synth_t<8>(p, q, qs, fm, fs, nf, s);
@@ -292,9 +347,9 @@ void ts_launch_leg_analys(ts_plan p, const float2 *g, long gs, float2 *q, long q
                           cudaStream_t s) {
   int K, W;
   pick_kw(p->nh, K, W);
-  // registers hold K*F complex pairs of weighted inputs: keep K*F <= 16
+  // registers hold K*F complex pairs of weighted inputs: keep K*F <= 24
   int F = nf >= 4 ? 4 : (nf >= 2 ? 2 : 1);
-  while (F > 1 && K * F > 16) F >>= 1;
+  while (F > 1 && K * F > 24) F >>= 1;
   if (F == 4) return leg_analys_f<4>(p, K, W, g, gs, q, qs, nf, s);
   if (F == 2) return leg_analys_f<2>(p, K, W, g, gs, q, qs, nf, s);
   return leg_analys_f<1>(p, K, W, g, gs, q, qs, nf, s);
