@@ -100,8 +100,14 @@ typedef struct ts_plan_info {
   int fourier;    /* TS_FOURIER_FFT or TS_FOURIER_DFT in use */
   int fft_stages; /* Stockham stages of the nphi/2-point FFT (0 for DFT) */
   int fft_radix[16];
+  long table_bytes; /* tensor-core P tables in device memory (0 for FP32) */
 } ts_plan_info;
 int ts_sht_plan_info(ts_plan plan, ts_plan_info *info);
+
+/* Synchronises the context's stream, then reports TS_ERR_TIMEOUT (and clears
+ * the flag) if a tensor-core kernel of this plan gave up a bounded wait for its
+ * MMAs since the last call; TS_OK otherwise. */
+int ts_sht_plan_status(ts_plan plan);
 
 /* Nodes x_i = cos(theta_i) (decreasing) and Gauss weights w_i, f64, nlat each,
  * as computed on the GPU (ShtPlan.cosTheta / gaussWeights, sht.ts:120-125). */
@@ -210,13 +216,15 @@ int ts_model_counts(ts_model model, int which, int *kernels, int *launches);
 /* Everything ts_model_compile does short of the GPU — parse, specialise,
  * schedule, generate CUDA C and compile it with NVRTC for sm_100a — for a grid
  * given by its sizes (no context, no device).  `describe` receives the
- * describe() text of init and step separated by a "====" line; `kernels` and
+ * describe() text of init and step separated by a "====" line; flags selects
+ * the precision (TS_PREC_*) whose kernels are generated; `kernels` and
  * `launches` are those of step.  For host-side checks of a model source
  * (the editor's compile-on-type, src/editor/, and the tests). */
 int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
                    const char *const *state, int nstate, const char *const *view, int nview,
-                   const char *const *params, int nparams, int batch, char *describe,
-                   size_t cap, int *kernels, int *launches, ts_compile_error *err);
+                   const char *const *params, int nparams, int batch, int flags,
+                   char *describe, size_t cap, int *kernels, int *launches,
+                   ts_compile_error *err);
 
 /* Seeding (src/mgpu/noise.ts:15-51; bench-sht.ts:132-144): mulberry32 and
  * Box-Muller, bit-identical integer state to the reference's.  amp-scaled

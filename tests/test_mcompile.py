@@ -8,14 +8,15 @@ from turing_sphere_b200 import _lib, mModels, defaultParams
 from turing_sphere_b200.model import formatFailure, ModelCompileError
 
 
-def check(source, state=("U",), view=("u",), params=(), lmax=15, nlat=16, nphi=32, batch=1):
+def check(source, state=("U",), view=("u",), params=(), lmax=15, nlat=16, nphi=32, batch=1,
+          precision=0):
     buf = C.create_string_buffer(1 << 16)
     k, n = C.c_int(), C.c_int()
     err = _lib.CompileError()
     rc = _lib.lib().ts_model_check(lmax, lmax, nlat, nphi, source.encode(),
                                    _lib.cstr_array(list(state)), len(state),
                                    _lib.cstr_array(list(view)), len(view),
-                                   _lib.cstr_array(list(params)), len(params), batch, buf,
+                                   _lib.cstr_array(list(params)), len(params), batch, precision, buf,
                                    len(buf), C.byref(k), C.byref(n), C.byref(err))
     if rc != _lib.TS_OK:
         raise ModelCompileError(err.message.decode(), err.start, err.end, err.fn.decode())
@@ -41,10 +42,13 @@ def test_models_fuse_one_kernel_per_line(model):
 
 
 @pytest.mark.parametrize("grid", [(63, 96, 192), (255, 384, 768), (127, 192, 384)])
-def test_schnakenberg_compiles_on_large_grids(grid):
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp32", "tf32x3"])
+def test_schnakenberg_compiles_on_large_grids(grid, precision):
     m = mModels[0]
     lmax, nlat, nphi = grid
-    check(m.source, m.state, m.species, [p.key for p in m.params], lmax, nlat, nphi, batch=64)
+    k, n, init, step = check(m.source, m.state, m.species, [p.key for p in m.params], lmax, nlat,
+                             nphi, batch=64, precision=precision)
+    assert n == 3
 
 
 LINEAR = open(__file__.replace("test_mcompile.py", "models/linear.m")).read()

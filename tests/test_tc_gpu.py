@@ -1,0 +1,79 @@
+"""The tcgen05 split-TF32 tensor-core Legendre path, through the C ABI, against
+the f64 oracle.  Tolerance: relative L2 per transform <= 1e-5."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from turing_sphere_b200 import ShtConfig, ShtPlan
+
+from .test_sht_gpu import scaled_spectrum
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def tc_plan(device, lmax, nlat, nphi, mmax=None):
+    mmax = lmax if mmax is None else mmax
+    return ShtPlan.create(device, ShtConfig(lmax, mmax, nlat, nphi), {"precision": "tf32x3"})
+
+
+@pytest.mark.parametrize("lmax,nlat,nphi,mmax,batch", [
+    (15, 16, 32, 15, 1),          # smallest tiles (N = 16)
+    (31, 32, 64, 31, 1),          # the reference transformChecks grid
+    (63, 96, 192, 63, 3),
+    (127, 192, 384, 127, 70),     # two 64-field blocks, the second partial
+    (255, 384, 768, 255, 2),      # one 192-latitude tile
+    (31, 33, 64, 31, 2),          # odd nlat: the equator row
+    (40, 48, 96, 20, 5),          # mmax < lmax
+])
+def test_tc_parity_with_oracle(device, lmax, nlat, nphi, mmax, batch):
+    plan = tc_plan(device, lmax, nlat, nphi, mmax)
+    assert plan.precision == "tf32x3" and plan.tableBytes > 0
+    ref = O.ShtReference(lmax, mmax, nlat, nphi)
+    qs = np.stack([scaled_spectrum(lmax, mmax, 20 + b) for b in range(batch)])
+    sp = plan.synth(qs, batch=batch).reshape(batch, -1)
+    plan.status()
+    for b in sorted({0, batch - 1}):
+        s_cpu = ref.synth(qs[b].astype(np.float64))
+        e_s = O.rel_l2(sp[b], s_cpu)
+        s32 = s_cpu.astype(np.float32)
+        e_a = O.rel_l2(plan.analys(s32), ref.analys(s32.astype(np.float64)))
+        assert e_s < TOL and e_a < TOL, (b, e_s, e_a)
+    back = plan.analys(sp, batch=batch).reshape(batch, -1)
+    plan.status()
+    assert O.rel_l2(back, qs) < TOL
+
+
+def test_tc_latitude_tiles_lmax511(device):
+    """nh = 384 latitudes: two 192-latitude tiles in the synthesis."""
+    lmax, nlat, nphi = 511, 768, 1536
+    plan = tc_plan(device, lmax, nlat, nphi)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = scaled_spectrum(lmax, lmax, 9)
+    s_cpu = ref.synth(q.astype(np.float64))
+    assert O.rel_l2(plan.synth(q), s_cpu) < TOL
+    s32 = s_cpu.astype(np.float32)
+    assert O.rel_l2(plan.analys(s32), ref.analys(s32.astype(np.float64))) < TOL
+    plan.status()
+
+
+@pytest.mark.parametrize("lmax,nlat,nphi", [(127, 192, 384), (255, 384, 768)])
+def test_tc_and_plain_both_within_tolerance(device, lmax, nlat, nphi):
+    """Both precisions against f64 on the same input; they agree with each
+    other to the sum of their errors."""
+    a = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi))
+    b = tc_plan(device, lmax, nlat, nphi)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = scaled_spectrum(lmax, lmax, 4)
+    s64 = ref.synth(q.astype(np.float64))
+    sa, sb = a.synth(q), b.synth(q)
+    ea, eb = O.rel_l2(sa, s64), O.rel_l2(sb, s64)
+    print(f"synth relL2 vs f64: fp32 {ea:.2e}, tf32x3 {eb:.2e}")
+    assert ea < TOL and eb < TOL
+    assert O.rel_l2(sb, sa) < ea + eb + 1e-7
+    s32 = s64.astype(np.float32)
+    q64 = ref.analys(s32.astype(np.float64))
+    fa, fb = O.rel_l2(a.analys(s32), q64), O.rel_l2(b.analys(s32), q64)
+    print(f"analys relL2 vs f64: fp32 {fa:.2e}, tf32x3 {fb:.2e}")
+    assert fa < TOL and fb < TOL

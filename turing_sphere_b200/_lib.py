@@ -48,7 +48,7 @@ class PlanInfo(C.Structure):
     _fields_ = [
         ("lmax", C.c_int), ("mmax", C.c_int), ("nlat", C.c_int), ("nphi", C.c_int),
         ("nlm", C.c_long), ("precision", C.c_int), ("fourier", C.c_int),
-        ("fft_stages", C.c_int), ("fft_radix", C.c_int * 16),
+        ("fft_stages", C.c_int), ("fft_radix", C.c_int * 16), ("table_bytes", C.c_long),
     ]
 
 
@@ -81,6 +81,7 @@ SIGNATURES = {
     "ts_sht_plan_destroy": (i32, [vp]),
     "ts_sht_plan_info": (i32, [vp, C.POINTER(PlanInfo)]),
     "ts_sht_plan_nodes": (i32, [vp, f64p, f64p]),
+    "ts_sht_plan_status": (i32, [vp]),
     "ts_sht_synth_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_analys_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_synth_noalloc": (i32, [vp, vp, vp, i32, vp]),
@@ -106,7 +107,7 @@ SIGNATURES = {
     "ts_model_source": (i32, [vp, C.c_char_p, C.c_size_t]),
     "ts_model_counts": (i32, [vp, i32, C.POINTER(i32), C.POINTER(i32)]),
     "ts_model_check": (i32, [i32, i32, i32, i32, cstr, C.POINTER(cstr), i32, C.POINTER(cstr), i32,
-                             C.POINTER(cstr), i32, i32, C.c_char_p, C.c_size_t, C.POINTER(i32),
+                             C.POINTER(cstr), i32, i32, i32, C.c_char_p, C.c_size_t, C.POINTER(i32),
                              C.POINTER(i32), C.POINTER(CompileError)]),
     "ts_seeded_noise": (None, [i64, C.c_double, C.c_uint, f32p]),
     "ts_seeded_spectrum": (None, [i32, i32, C.c_uint, f32p]),

@@ -84,6 +84,7 @@ void plan_free(ts_plan p) {
   p->fm.release();
   p->stage_q.release();
   p->stage_s.release();
+  ts_tc_free(p);
 }
 
 void check_batch(ts_plan p, const void *a, const void *b, int batch) {
@@ -255,9 +256,9 @@ int ts_sht_plan_create(ts_ctx ctx, int lmax, int mmax, int nlat, int nphi, int f
     p->fourier = (want == TS_FOURIER_DFT || !fft_ok) ? TS_FOURIER_DFT : TS_FOURIER_FFT;
     if (p->fourier == TS_FOURIER_DFT) p->fft.nst = 0;
     ts_init_tables(p);
-    if (p->precision != TS_PREC_FP32) {
-      ts_throw(TS_ERR_UNSUPPORTED, "tensor-core precision is not built into this library yet");
-    }
+    if (p->precision == TS_PREC_BF16X3)
+      ts_throw(TS_ERR_UNSUPPORTED, "split-BF16 tensor-core Legendre is not built; use TF32x3");
+    if (p->precision == TS_PREC_TF32X3) ts_tc_init(p);
     *out = p;
     return TS_OK;
   } catch (const ts_exc &e) {
@@ -290,8 +291,23 @@ int ts_sht_plan_info(ts_plan p, ts_plan_info *info) {
   info->precision = p->precision;
   info->fourier = p->fourier;
   info->fft_stages = p->fourier == TS_FOURIER_FFT ? p->fft.nst : 0;
+  info->table_bytes = (long)ts_tc_bytes(p);
   for (int i = 0; i < info->fft_stages; i++) info->fft_radix[i] = p->fft.radix[i];
   return TS_OK;
+}
+
+int ts_sht_plan_status(ts_plan p) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
+  TS_CUDA(cudaSetDevice(ctx->device));
+  TS_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ts_tc_check_error(p)) {
+    int zero = 0;
+    TS_CUDA(cudaMemcpy(ts_tc_tab(p).err, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    ts_throw(TS_ERR_TIMEOUT, "a tensor-core kernel gave up waiting for its MMAs");
+  }
+  TS_API_END(ctx)
 }
 
 int ts_sht_plan_nodes(ts_plan p, double *cos_theta, double *weights) {

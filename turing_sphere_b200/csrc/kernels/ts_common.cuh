@@ -95,6 +95,18 @@ struct TsFftTab {
   int radix[16];
 };
 
+// Tensor-core Legendre tables of a plan (see leg_tc.cuh).
+struct TsTcTab {
+  const char *synth;        // synthesis image
+  const long *synth_off;    // byte offset of each m's block, mmax+1 entries
+  const char *anal;         // analysis image
+  const long *anal_off;
+  int NL, nLT;              // synthesis latitude tile (N of the MMA) and tile count
+  int LTL;                  // analysis l-tile (per parity), <= 256
+  int nLC;                  // analysis latitude chunks of 32
+  int *err;                 // set to 1 when a bounded wait gives up
+};
+
 // Grid-phase I/O of a compiled model (see ts_fourier_phase in fourier.cuh).
 struct TsPhaseIO {
   const float2 *fm;

@@ -29,6 +29,8 @@
 #include "mlang.h"
 #include "runtime.h"
 
+#define TS_TC_FIELDS 64  // fields per tensor-core CTA (kernels/leg_tc.cuh)
+
 using tsm::Dom;
 
 namespace {
@@ -459,7 +461,15 @@ void schedule(ts_model m, Program &P, bool is_step) {
     st.nana = (int)A.size();
     for (int v : sin) st.in.push_back(ref[v]);
     for (int v : sout) st.out.push_back(ref[v]);
-    ts_analys_shape(p, m->batch * st.nana, st.nana, &st.F, &st.K, &st.W, &st.per_cta);
+    const bool tc = p->precision != TS_PREC_FP32;
+    if (tc) {
+      st.per_cta = st.nana * (TS_TC_FIELDS / st.nana);  // whole instances per 64-field block
+      if (st.per_cta == 0)
+        throw tsm::CompileError{"too many analys outputs per instance for the tensor-core path",
+                                -1, -1, f.name};
+    } else {
+      ts_analys_shape(p, m->batch * st.nana, st.nana, &st.F, &st.K, &st.W, &st.per_cta);
+    }
     Emitter em{f, {}};
     const std::string en = "TsEpi_" + ptag + std::to_string(tag++);
     std::ostringstream src;
@@ -498,8 +508,9 @@ void schedule(ts_model m, Program &P, bool is_step) {
       src << "      io.sout[" << o << "][inst * io.sout_stride[" << o << "] + idx] = v"
           << sout[o] << ";\n";
     src << "    }\n  }\n};\n";
-    st.expr = "ts_leg_analys_f32<" + std::to_string(st.F) + ", " + std::to_string(st.K) + ", 2, " +
-              en + ">";
+    st.expr = tc ? "ts_leg_analys_tc<" + en + ">"
+                 : "ts_leg_analys_f32<" + std::to_string(st.F) + ", " + std::to_string(st.K) +
+                       ", 2, " + en + ">";
     st.label = "legana  " + std::to_string(A.size()) + " field(s), " + std::to_string(E.size()) +
                " spectral statement(s) fused";
     st.src = src.str();
@@ -532,7 +543,8 @@ std::string stage_title(const Stage &s) { return s.label; }
 // and the lowered name of every template instantiation.
 std::vector<char> build_cubin(ts_model m, std::map<std::string, std::string> &lowered) {
   std::ostringstream src;
-  src << "#include \"ts_common.cuh\"\n#include \"fourier.cuh\"\n#include \"leg_f32.cuh\"\n";
+  src << "#include \"ts_common.cuh\"\n#include \"fourier.cuh\"\n#include \"leg_f32.cuh\"\n"
+      << "#include \"leg_tc.cuh\"\n";
   for (auto &P : m->prog)
     for (auto &s : P.stages) src << stage_source(s);
   const std::string code = src.str();
@@ -654,9 +666,16 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
         long gs = field;
         int nfields = B * s.nana;
         int per_cta = s.per_cta;
-        void *args[] = {&leg, &g, &gs, &epi, &nfields, &per_cta};
-        dim3 grid(p->mmax + 1, (nfields + per_cta - 1) / per_cta);
-        TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(32 * s.W), args, s.smem, st));
+        if (p->precision != TS_PREC_FP32) {
+          TsTcTab tc = ts_tc_tab(p);
+          void *args[] = {&leg, &tc, &g, &gs, &epi, &nfields, &per_cta};
+          dim3 grid((nfields + per_cta - 1) / per_cta, p->mmax + 1, 2 * ts_tc_ntile(p));
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(128), args, s.smem, st));
+        } else {
+          void *args[] = {&leg, &g, &gs, &epi, &nfields, &per_cta};
+          dim3 grid(p->mmax + 1, (nfields + per_cta - 1) / per_cta);
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(32 * s.W), args, s.smem, st));
+        }
         break;
       }
       case Stage::SpecEW: {
@@ -683,7 +702,7 @@ void finish_shapes(ts_model m) {
         const int nrows = s.nsyn + s.nana + 1;
         s.lb = ts_fourier_lb(p, m->batch, nrows, &s.smem);
       } else if (s.kind == Stage::LegAnalys) {
-        s.smem = ts_analys_smem(p, s.F, s.W);
+        s.smem = p->precision != TS_PREC_FP32 ? ts_tc_analys_smem(p) : ts_analys_smem(p, s.F, s.W);
       }
     }
 }
@@ -1061,8 +1080,9 @@ int ts_model_counts(ts_model m, int which, int *kernels, int *launches) {
 // line "====") to `describe` and the kernel and launch counts of step.
 int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
                    const char *const *state, int nstate, const char *const *view, int nview,
-                   const char *const *params, int nparams, int batch, char *describe,
-                   size_t cap, int *kernels, int *launches, ts_compile_error *err) {
+                   const char *const *params, int nparams, int batch, int flags,
+                   char *describe, size_t cap, int *kernels, int *launches,
+                   ts_compile_error *err) {
   if (err) memset(err, 0, sizeof(*err));
   ts_ctx_s ctx;
   ctx.sm_count = 148;
@@ -1081,6 +1101,7 @@ int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
     plan.nphi = nphi;
     plan.nh = (nlat + 1) / 2;
     plan.nlm = ts_nlm_calc(lmax, mmax);
+    plan.precision = flags & TS_PREC_MASK;
     plan.fft.nphi = nphi;
     plan.fft.H = nphi / 2;
     plan.fft.mmax = mmax;

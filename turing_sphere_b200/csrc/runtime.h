@@ -100,4 +100,18 @@ size_t ts_analys_smem(ts_plan p, int F, int W);
 // rows per Fourier CTA for a kernel holding `nrows` rows per warp
 int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem);
 void ts_init_tables(ts_plan p);
+// tensor-core tables and kernels (sht_tc.cu)
+struct TsTcTab;
+void ts_tc_init(ts_plan p);
+void ts_tc_free(ts_plan p);
+const TsTcTab &ts_tc_tab(ts_plan p);
+int ts_tc_ntile(ts_plan p);
+size_t ts_tc_bytes(ts_plan p);
+size_t ts_tc_synth_smem(ts_plan p);
+size_t ts_tc_analys_smem(ts_plan p);
+void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fm_stride, int nfields,
+                            cudaStream_t s);
+void ts_launch_leg_analys_tc(ts_plan p, const float2 *g, long g_stride, float2 *q, long q_stride,
+                             int nfields, cudaStream_t s);
+int ts_tc_check_error(ts_plan p);
 void ts_kernel_attrs_once(ts_ctx ctx);

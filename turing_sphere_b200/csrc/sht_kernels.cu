@@ -297,6 +297,7 @@ void ts_kernel_attrs_once(ts_ctx ctx) {
 
 void ts_launch_leg_synth_fields(ts_plan p, const TsFields &q, float2 *fm, long fs, int nf,
                                 cudaStream_t s) {
+  if (p->precision != TS_PREC_FP32) return ts_launch_leg_synth_tc(p, q, fm, fs, nf, s);
   const int bd = p->nh >= 128 ? 64 : 32;
   auto go = [&](auto Fc) {
     constexpr int F = decltype(Fc)::value;
@@ -337,6 +338,13 @@ int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem) {
 
 void ts_launch_leg_synth(ts_plan p, const float2 *q, long qs, float2 *fm, long fs, int nf,
                          cudaStream_t s) {
+  if (p->precision != TS_PREC_FP32) {
+    TsFields qf{};
+    qf.base[0] = q;
+    qf.inst_stride[0] = qs;
+    qf.nper = 1;
+    return ts_launch_leg_synth_tc(p, qf, fm, fs, nf, s);
+  }
   if (nf >= 8) return leg_synth_t<8>(p, q, qs, fm, fs, nf, s);
   if (nf >= 4) return leg_synth_t<4>(p, q, qs, fm, fs, nf, s);
   if (nf >= 2) return leg_synth_t<2>(p, q, qs, fm, fs, nf, s);
@@ -345,6 +353,7 @@ void ts_launch_leg_synth(ts_plan p, const float2 *q, long qs, float2 *fm, long f
 
 void ts_launch_leg_analys(ts_plan p, const float2 *g, long gs, float2 *q, long qs, int nf,
                           cudaStream_t s) {
+  if (p->precision != TS_PREC_FP32) return ts_launch_leg_analys_tc(p, g, gs, q, qs, nf, s);
   int K, W;
   pick_kw(p->nh, K, W);
   // registers hold K*F complex pairs of weighted inputs: keep K*F <= 24

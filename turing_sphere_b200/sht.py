@@ -82,6 +82,7 @@ class ShtPlan:
         self.fourierMode = "dft" if info.fourier == _lib.TS_FOURIER_DFT else "fft"
         self.precision = {v: k for k, v in PRECISIONS.items()}[info.precision]
         self.fftRadices = [info.fft_radix[i] for i in range(info.fft_stages)]
+        self.tableBytes = info.table_bytes
         x = np.zeros(cfg.nlat)
         w = np.zeros(cfg.nlat)
         _lib.check(_lib.lib().ts_sht_plan_nodes(handle, _lib.dptr(x), _lib.dptr(w)), device.handle)
@@ -145,6 +146,10 @@ class ShtPlan:
               "fourAnalys": "ts_sht_fourier_analys_dev", "legAnalys": "ts_sht_leg_analys_dev"}[stage]
         _lib.check(getattr(_lib.lib(), fn)(self.handle, src_ptr, dst_ptr, batch, stream),
                    self.device.handle)
+
+    def status(self) -> None:
+        """Raise TsError(TS_ERR_TIMEOUT) if a tensor-core kernel gave up a wait."""
+        _lib.check(_lib.lib().ts_sht_plan_status(self.handle), self.device.handle)
 
     def destroy(self) -> None:
         if self.handle:
