@@ -12,10 +12,12 @@
 // data operand (Q or W) is split on the fly: hi = rna_tf32(x),
 // lo = rna_tf32(x - hi); each k-step issues hi*hi + hi*lo + lo*hi.
 //
-// One elected thread issues the MMAs; tcgen05.commit signals an mbarrier per
-// shared-memory stage (two stages).  Every wait is bounded: on timeout the
-// kernel records an error flag, skips the epilogue, frees its tensor memory
-// and returns.
+// Warp roles (192 threads): warps 0-3 build the data operand of each stage
+// and run the epilogue (they own TMEM lanes 0-127), warp 4 streams the table
+// chunks with cp.async.bulk (expect-tx mbarrier), warp 5 issues the MMAs and
+// commits each stage back to its producers.  Every wait is bounded: on
+// timeout the kernel records an error flag, skips the epilogue, frees its
+// tensor memory and returns.
 #pragma once
 #include "ts_common.cuh"
 
@@ -172,13 +174,61 @@ TS_DEV long ts_atile_offset(const TsTcTab &tc, int lmax, int m, int par, int lti
   return off;
 }
 
+TS_DEV void ts_mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(ts_smem_u32(bar)) : "memory");
+}
+
+TS_DEV void ts_mbar_arrive_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ts_smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// global -> shared bulk copy (no multicast), completion counted on `bar`
+TS_DEV void ts_bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          ts_smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(ts_smem_u32(bar))
+      : "memory");
+}
+
+#define TS_TC_THREADS 192
+#define TS_TC_MAXSTAGE 4
+
+// Pipeline bookkeeping shared by both kernels: full[s] completes when the
+// table bytes of stage s have landed and the 4 producer warps have arrived;
+// empty[s] completes when the MMAs that read stage s are done; done[0] when
+// all MMAs are.
+struct TsTcPipe {
+  unsigned long long full[TS_TC_MAXSTAGE], empty[TS_TC_MAXSTAGE], done;
+  unsigned tmem;
+  int bad;
+};
+
+TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S) {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; s++) {
+      ts_mbar_init(&pp->full[s], 5);
+      ts_mbar_init(&pp->empty[s], 1);
+    }
+    ts_mbar_init(&pp->done, 1);
+    pp->bad = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+}
+
+TS_DEV void ts_tc_flag(TsTcPipe *pp) { atomicExch(&pp->bad, 1); }
+
 // ----------------------------------------------------------------- synthesis
 //
-// grid = (ceil(nfields/64), mmax+1, nLT), block = 128.  Dynamic shared memory:
-// 1024-aligned, max(2 stages x (2*NL*128 + 2*16384), 2*128*(NL+4)*4) + 64.
-__global__ void __launch_bounds__(128, 1)
+// grid = (ceil(nfields/64), mmax+1, nLT), block = 192.  Stages (2*16384 bytes
+// of data operand + 2*NL*128 bytes of table each) cycle through the k chunks
+// of both parities, interleaved.  Dynamic shared memory: S*stage + 1024 +
+// sizeof(TsTcPipe).
+__global__ void __launch_bounds__(TS_TC_THREADS, 1)
 ts_leg_synth_tc(TsLegTab t, TsTcTab tc, TsFields q, float2 *__restrict__ fm, long fm_stride,
-                int nfields) {
+                int nfields, int S) {
   extern __shared__ __align__(1024) char ts_smem_st[];
   char *smem = (char *)(((unsigned long long)ts_smem_st + 1023) & ~1023ull);
   const int fb = blockIdx.x, m = blockIdx.y, lt = blockIdx.z;
@@ -187,129 +237,159 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, TsFields q, float2 *__restrict__ fm, lon
   const long base = ts_lm_base(t.lmax, m);
   const int kp0 = ts_kpar(t.lmax, m, 0), kp1 = ts_kpar(t.lmax, m, 1);
   const int nch0 = (kp0 + TS_TC_KCH - 1) / TS_TC_KCH, nch1 = (kp1 + TS_TC_KCH - 1) / TS_TC_KCH;
-  const int C = nch0 + nch1;
-  const int bbytes = NL * 128;                     // one B image (hi or lo)
-  const int stage = 2 * bbytes + 2 * 16384;        // B hi, B lo, A hi, A lo
-  const int SP = NL + 1;  // staging row pitch (floats), odd: conflict-free
-  const int stage_all = max(2 * stage, 2 * TS_TC_ROWS * SP * 4);
-  unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem + stage_all);
-  unsigned *slot = reinterpret_cast<unsigned *>(smem + stage_all + 16);
+  const int T = nch0 + nch1;
+  const int bbytes = NL * 128;
+  const int stage = 2 * 16384 + 2 * bbytes;  // A hi, A lo, B hi, B lo
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage);
   const unsigned ncols = ts_tmem_cols(2 * NL);
+  // chunk t -> (parity, chunk of that parity): parities interleaved
+  auto chunk = [&](int t_, int &par, int &cc) {
+    const int both = 2 * min(nch0, nch1);
+    if (t_ < both) {
+      par = t_ & 1;
+      cc = t_ >> 1;
+    } else {
+      par = nch0 > nch1 ? 0 : 1;
+      cc = (t_ - both) + min(nch0, nch1);
+    }
+  };
 
-  if (tid == 0) {
-    ts_mbar_init(&bars[0], 1);
-    ts_mbar_init(&bars[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 0) ts_tmem_alloc(slot, ncols);
+  ts_tc_pipe_init(pp, S);
+  if (warp == 0) ts_tmem_alloc(&pp->tmem, ncols);
   ts_tc_fence_before();
   __syncthreads();
   ts_tc_fence_after();
-  const unsigned tmem = *slot;
-  const unsigned idesc = ts_idesc_tf32(NL);
-  bool ok = true;
+  const unsigned tmem = pp->tmem;
 
-  for (int c = 0; c < C && ok; c++) {
-    const int b = c & 1;
-    char *sb = smem + b * stage;
-    if (c >= 2) ok = ts_mbar_wait(&bars[b], ((c >> 1) - 1) & 1, TS_TC_WAIT_LIMIT);
-    if (!__syncthreads_and(ok)) {
-      ok = false;
-      break;
-    }
-    const int par = c < nch0 ? 0 : 1;
-    const int cc = par ? c - nch0 : c;
-    // P image chunk (hi then lo), laid out exactly as the MMA reads it
-    const long src = tc.synth_off[m] + (long)((par ? nch0 : 0) + cc) * tc.nLT * 2 * bbytes +
-                     (long)lt * 2 * bbytes;
-    ts_copy16(sb, tc.synth + src, 2 * bbytes);
-    // Q chunk split into hi/lo: thread -> (field, 16 consecutive k)
-    {
-      const int fl = tid & 63, kh = tid >> 6;
-      const int f = fb * TS_TC_FIELDS + fl;
-      const float2 *qf = f < nfields ? ts_field(q, f) + base : nullptr;
-      char *ahi = sb + 2 * bbytes, *alo = ahi + 16384;
+  if (warp < 4) {
+    // ---- data operand producers: Q split into TF32 hi/lo, 16 k per thread
+    const int fl = tid & 63, kh = tid >> 6;
+    const int f = fb * TS_TC_FIELDS + fl;
+    const float2 *qf = f < nfields ? ts_field(q, f) + base : nullptr;
+    for (int t_ = 0; t_ < T; t_++) {
+      const int s = t_ % S, use = t_ / S;
+      int par, cc;
+      chunk(t_, par, cc);
+      float2 v[16];
+      const int kp = par ? kp1 : kp0;
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int j = cc * TS_TC_KCH + kh * 16 + u;
+        v[u] = (qf && j < kp) ? qf[par + 2 * j] : make_float2(0.f, 0.f);
+      }
+      if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
+        ts_tc_flag(pp);
+        break;
+      }
+      char *ahi = smem + s * stage, *alo = ahi + 16384;
 #pragma unroll
       for (int k4 = 0; k4 < 4; k4++) {
-        float re[4], im[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int j = cc * TS_TC_KCH + kh * 16 + k4 * 4 + u;
-          float2 v = make_float2(0.f, 0.f);
-          if (qf && j < (par ? kp1 : kp0)) v = qf[par + 2 * j];
-          re[u] = v.x;
-          im[u] = v.y;
-        }
         const int k = kh * 16 + k4 * 4;
         float4 h, l;
-        h = make_float4(ts_rna_tf32(re[0]), ts_rna_tf32(re[1]), ts_rna_tf32(re[2]), ts_rna_tf32(re[3]));
-        l = make_float4(ts_rna_tf32(re[0] - h.x), ts_rna_tf32(re[1] - h.y), ts_rna_tf32(re[2] - h.z),
-                        ts_rna_tf32(re[3] - h.w));
+        h = make_float4(ts_rna_tf32(v[4 * k4].x), ts_rna_tf32(v[4 * k4 + 1].x),
+                        ts_rna_tf32(v[4 * k4 + 2].x), ts_rna_tf32(v[4 * k4 + 3].x));
+        l = make_float4(ts_rna_tf32(v[4 * k4].x - h.x), ts_rna_tf32(v[4 * k4 + 1].x - h.y),
+                        ts_rna_tf32(v[4 * k4 + 2].x - h.z), ts_rna_tf32(v[4 * k4 + 3].x - h.w));
         *reinterpret_cast<float4 *>(ahi + ts_swz(2 * fl, k)) = h;
         *reinterpret_cast<float4 *>(alo + ts_swz(2 * fl, k)) = l;
-        h = make_float4(ts_rna_tf32(im[0]), ts_rna_tf32(im[1]), ts_rna_tf32(im[2]), ts_rna_tf32(im[3]));
-        l = make_float4(ts_rna_tf32(im[0] - h.x), ts_rna_tf32(im[1] - h.y), ts_rna_tf32(im[2] - h.z),
-                        ts_rna_tf32(im[3] - h.w));
+        h = make_float4(ts_rna_tf32(v[4 * k4].y), ts_rna_tf32(v[4 * k4 + 1].y),
+                        ts_rna_tf32(v[4 * k4 + 2].y), ts_rna_tf32(v[4 * k4 + 3].y));
+        l = make_float4(ts_rna_tf32(v[4 * k4].y - h.x), ts_rna_tf32(v[4 * k4 + 1].y - h.y),
+                        ts_rna_tf32(v[4 * k4 + 2].y - h.z), ts_rna_tf32(v[4 * k4 + 3].y - h.w));
         *reinterpret_cast<float4 *>(ahi + ts_swz(2 * fl + 1, k)) = h;
         *reinterpret_cast<float4 *>(alo + ts_swz(2 * fl + 1, k)) = l;
       }
+      ts_fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) ts_mbar_arrive(&pp->full[s]);
     }
-    ts_fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      ts_tc_fence_after();
-      const unsigned bhi = ts_smem_u32(sb), blo = bhi + bbytes;
-      const unsigned ahi = bhi + 2 * bbytes, alo = ahi + 16384;
-      const unsigned d = tmem + (unsigned)(par * NL);
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) {
-        const unsigned acc = (cc > 0 || kk > 0) ? 1u : 0u;
-        ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, acc);
-        ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(blo + kk * 32), idesc, 1u);
-        ts_mma_tf32(d, ts_umma_desc(alo + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, 1u);
+  } else if (warp == 4) {
+    // ---- table stream
+    if (lane == 0) {
+      for (int t_ = 0; t_ < T; t_++) {
+        const int s = t_ % S, use = t_ / S;
+        int par, cc;
+        chunk(t_, par, cc);
+        if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
+          ts_tc_flag(pp);
+          break;
+        }
+        const long src = tc.synth_off[m] + (long)((par ? nch0 : 0) + cc) * tc.nLT * 2 * bbytes +
+                         (long)lt * 2 * bbytes;
+        ts_mbar_arrive_tx(&pp->full[s], 2 * bbytes);
+        ts_bulk_g2s(smem + s * stage + 2 * 16384, tc.synth + src, 2 * bbytes, &pp->full[s]);
       }
-      ts_mma_commit(&bars[b]);
+    }
+  } else {
+    // ---- MMA issue
+    if (lane == 0) {
+      const unsigned idesc = ts_idesc_tf32(NL);
+      for (int t_ = 0; t_ < T; t_++) {
+        const int s = t_ % S, use = t_ / S;
+        int par, cc;
+        chunk(t_, par, cc);
+        if (!ts_mbar_wait(&pp->full[s], use & 1, TS_TC_WAIT_LIMIT)) {
+          ts_tc_flag(pp);
+          break;
+        }
+        ts_tc_fence_after();
+        const unsigned ahi = ts_smem_u32(smem + s * stage), alo = ahi + 16384;
+        const unsigned bhi = ahi + 2 * 16384, blo = bhi + bbytes;
+        const unsigned d = tmem + (unsigned)(par * NL);
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+          const unsigned acc = (cc > 0 || kk > 0) ? 1u : 0u;
+          ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, acc);
+          ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(blo + kk * 32), idesc, 1u);
+          ts_mma_tf32(d, ts_umma_desc(alo + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, 1u);
+        }
+        ts_mma_commit(&pp->empty[s]);
+      }
+      ts_mma_commit(&pp->done);
     }
   }
-  // all MMAs done once the last commit has landed
-  if (ok && C > 0) ok = ts_mbar_wait(&bars[(C - 1) & 1], ((C - 1) >> 1) & 1, TS_TC_WAIT_LIMIT);
-  ok = __syncthreads_and(ok);
-  ts_tc_fence_after();
-  if (ok) {
-    // TMEM -> shared staging sE/sO[row][NL+4]
-    float *sE = reinterpret_cast<float *>(smem);
-    float *sO = sE + TS_TC_ROWS * SP;
-    const int row = warp * 32 + lane;
-    for (int c0 = 0; c0 < NL; c0 += 16) {
-      float v[16];
-      ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
+
+  // ---- epilogue (warps 0-3 own TMEM lanes 0-127): rows 2f (re) and 2f+1 (im)
+  // sit in adjacent lanes; each pair swaps halves so that every thread writes
+  // 8 consecutive complex values, north and (mirrored) south
+  if (warp < 4) {
+    bool ok = ts_mbar_wait(&pp->done, 0, TS_TC_WAIT_LIMIT) && !pp->bad;
+    ts_tc_fence_after();
+    const int fl = (warp * 32 + lane) >> 1, comp = lane & 1;
+    const int f = fb * TS_TC_FIELDS + fl;
+    float2 *dst = fm + (long)f * fm_stride + (long)m * t.nlat;
+    if (ok) {
+      for (int c0 = 0; c0 < NL; c0 += 16) {
+        float e[16], o[16];
+        ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, e);
+        if (nch1 > 0)
+          ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(NL + c0), o);
+        else
 #pragma unroll
-      for (int i = 0; i < 16; i++) sE[row * SP + c0 + i] = v[i];
-      if (nch1 > 0) {
-        ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(NL + c0), v);
+          for (int i = 0; i < 16; i++) o[i] = 0.f;
+        // re-lane keeps columns 0-7 and takes the partner's im; im-lane 8-15
+        float2 en[8], on[8];
 #pragma unroll
-        for (int i = 0; i < 16; i++) sO[row * SP + c0 + i] = v[i];
-      } else {
+        for (int i = 0; i < 8; i++) {
+          const float se = __shfl_xor_sync(0xffffffffu, comp ? e[i] : e[8 + i], 1);
+          const float so = __shfl_xor_sync(0xffffffffu, comp ? o[i] : o[8 + i], 1);
+          en[i] = comp ? make_float2(se, e[8 + i]) : make_float2(e[i], se);
+          on[i] = comp ? make_float2(so, o[8 + i]) : make_float2(o[i], so);
+        }
+        if (f < nfields) {
 #pragma unroll
-        for (int i = 0; i < 16; i++) sO[row * SP + c0 + i] = 0.f;
+          for (int i = 0; i < 8; i++) {
+            const int lat = lt * NL + c0 + comp * 8 + i;
+            if (lat < t.nh) {
+              dst[lat] = make_float2(en[i].x + on[i].x, en[i].y + on[i].y);
+              const int south = t.nlat - 1 - lat;
+              if (south != lat) dst[south] = make_float2(en[i].x - on[i].x, en[i].y - on[i].y);
+            }
+          }
+        }
       }
     }
-    ts_tc_fence_before();
-    __syncthreads();
-    for (int idx = tid; idx < TS_TC_FIELDS * NL; idx += blockDim.x) {
-      const int fl = idx / NL, j = idx - fl * NL;
-      const int f = fb * TS_TC_FIELDS + fl;
-      const int lat = lt * NL + j;
-      if (f >= nfields || lat >= t.nh) continue;
-      const float er = sE[(2 * fl) * SP + j], ei = sE[(2 * fl + 1) * SP + j];
-      const float orr = sO[(2 * fl) * SP + j], oi = sO[(2 * fl + 1) * SP + j];
-      float2 *dst = fm + (long)f * fm_stride + (long)m * t.nlat;
-      dst[lat] = make_float2(er + orr, ei + oi);
-      const int south = t.nlat - 1 - lat;
-      if (south != lat) dst[south] = make_float2(er - orr, ei - oi);
-    }
-  } else if (tid == 0) {
-    atomicExch(tc.err, 1);
+    if (!ok && tid == 0) atomicExch(tc.err, 1);
   }
   ts_tc_fence_before();
   __syncthreads();
@@ -318,14 +398,14 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, TsFields q, float2 *__restrict__ fm, lon
 
 // ------------------------------------------------------------------ analysis
 //
-// grid = (ceil(nfields/per_cta), mmax+1, 2*ntile), block = 128; z = par*ntile
-// + ltile (empty tiles return at once).  per_cta <= 64 fields.  Dynamic
-// shared memory: 1024-aligned, max(2 stages x (2*16384 + 2*N*128),
-// N*2*64*4) + 64, N <= LTL.
+// grid = (ceil(nfields/per_cta), mmax+1, 2*ntile), block = 192; z = par*ntile
+// + ltile (empty tiles return at once).  per_cta <= 64 fields.  Stages: 2*16384
+// bytes of data operand + 2*N*128 bytes of table, over the latitude chunks.
+// Dynamic shared memory: max(S*stage, N*2*64*4) + 1024 + sizeof(TsTcPipe).
 template <class Epi>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(TS_TC_THREADS, 1)
 ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const float2 *__restrict__ g, long g_stride, Epi epi,
-                 int nfields, int per_cta) {
+                 int nfields, int per_cta, int S) {
   extern __shared__ __align__(1024) char ts_smem_at[];
   char *smem = (char *)(((unsigned long long)ts_smem_at + 1023) & ~1023ull);
   const int m = blockIdx.y;
@@ -339,93 +419,118 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const float2 *__restrict__ g, long g_st
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long base = ts_lm_base(t.lmax, m);
   const int bbytes = N * 128;
-  const int stage = 2 * 16384 + 2 * bbytes;  // A hi, A lo, B hi, B lo
-  const int stage_all = max(2 * stage, N * 2 * TS_TC_FIELDS * 4);
-  unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem + stage_all);
-  unsigned *slot = reinterpret_cast<unsigned *>(smem + stage_all + 16);
+  const int stage = 2 * 16384 + 2 * bbytes;
+  const int region = max(S * stage, N * 2 * TS_TC_FIELDS * 4);
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + region);
   const unsigned ncols = ts_tmem_cols(N);
   const long toff = ts_atile_offset(tc, t.lmax, m, par, ltile);
-  const int C = tc.nLC;
+  const int T = tc.nLC;
 
-  if (tid == 0) {
-    ts_mbar_init(&bars[0], 1);
-    ts_mbar_init(&bars[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 0) ts_tmem_alloc(slot, ncols);
+  ts_tc_pipe_init(pp, S);
+  if (warp == 0) ts_tmem_alloc(&pp->tmem, ncols);
   ts_tc_fence_before();
   __syncthreads();
   ts_tc_fence_after();
-  const unsigned tmem = *slot;
-  const unsigned idesc = ts_idesc_tf32(N);
-  bool ok = true;
+  const unsigned tmem = pp->tmem;
 
-  for (int c = 0; c < C && ok; c++) {
-    const int b = c & 1;
-    char *sb = smem + b * stage;
-    if (c >= 2) ok = ts_mbar_wait(&bars[b], ((c >> 1) - 1) & 1, TS_TC_WAIT_LIMIT);
-    if (!__syncthreads_and(ok)) {
-      ok = false;
-      break;
-    }
-    ts_copy16(sb + 2 * 16384, tc.anal + toff + (long)c * 2 * bbytes, 2 * bbytes);
-    // W chunk: thread -> (latitude k of the chunk, 16 fields)
-    {
-      const int k = tid & 31, fg = tid >> 5;
+  if (warp < 4) {
+    // ---- data operand: W = w (G_north +- G_south), lane = latitude of the chunk
+    const int k = lane, fg = warp;
+    for (int c = 0; c < T; c++) {
+      const int s = c % S, use = c / S;
       const int lat = c * TS_TC_KCH + k;
       const bool live = lat < t.nh;
       const float w = live ? t.wq[lat] : 0.f;
       const int south = t.nlat - 1 - lat;
-      char *ahi = sb, *alo = sb + 16384;
-#pragma unroll 4
+      float2 gn[16], gs[16];
+#pragma unroll
       for (int i = 0; i < 16; i++) {
         const int fl = fg * 16 + i;
-        float2 gn = make_float2(0.f, 0.f), gs = make_float2(0.f, 0.f);
+        gn[i] = gs[i] = make_float2(0.f, 0.f);
         if (live && fl < nf) {
           const float2 *src = g + (long)(f0 + fl) * g_stride + (long)m * t.nlat;
-          gn = src[lat];
-          if (south != lat) gs = src[south];
+          gn[i] = src[lat];
+          if (south != lat) gs[i] = src[south];
         }
-        const float wr = par ? (gn.x - gs.x) * w : (gn.x + gs.x) * w;
-        const float wi = par ? (gn.y - gs.y) * w : (gn.y + gs.y) * w;
+      }
+      if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
+        ts_tc_flag(pp);
+        break;
+      }
+      char *ahi = smem + s * stage, *alo = ahi + 16384;
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        const int fl = fg * 16 + i;
+        const float wr = par ? (gn[i].x - gs[i].x) * w : (gn[i].x + gs[i].x) * w;
+        const float wi = par ? (gn[i].y - gs[i].y) * w : (gn[i].y + gs[i].y) * w;
         const float hr = ts_rna_tf32(wr), hi = ts_rna_tf32(wi);
         *reinterpret_cast<float *>(ahi + ts_swz(2 * fl, k)) = hr;
         *reinterpret_cast<float *>(alo + ts_swz(2 * fl, k)) = ts_rna_tf32(wr - hr);
         *reinterpret_cast<float *>(ahi + ts_swz(2 * fl + 1, k)) = hi;
         *reinterpret_cast<float *>(alo + ts_swz(2 * fl + 1, k)) = ts_rna_tf32(wi - hi);
       }
+      ts_fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) ts_mbar_arrive(&pp->full[s]);
     }
-    ts_fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      ts_tc_fence_after();
-      const unsigned ahi = ts_smem_u32(sb), alo = ahi + 16384;
-      const unsigned bhi = ahi + 2 * 16384, blo = bhi + bbytes;
-#pragma unroll
-      for (int kk = 0; kk < 4; kk++) {
-        const unsigned acc = (c > 0 || kk > 0) ? 1u : 0u;
-        ts_mma_tf32(tmem, ts_umma_desc(ahi + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, acc);
-        ts_mma_tf32(tmem, ts_umma_desc(ahi + kk * 32), ts_umma_desc(blo + kk * 32), idesc, 1u);
-        ts_mma_tf32(tmem, ts_umma_desc(alo + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, 1u);
+  } else if (warp == 4) {
+    if (lane == 0) {
+      for (int c = 0; c < T; c++) {
+        const int s = c % S, use = c / S;
+        if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
+          ts_tc_flag(pp);
+          break;
+        }
+        ts_mbar_arrive_tx(&pp->full[s], 2 * bbytes);
+        ts_bulk_g2s(smem + s * stage + 2 * 16384, tc.anal + toff + (long)c * 2 * bbytes,
+                    2 * bbytes, &pp->full[s]);
       }
-      ts_mma_commit(&bars[b]);
+    }
+  } else {
+    if (lane == 0) {
+      const unsigned idesc = ts_idesc_tf32(N);
+      for (int c = 0; c < T; c++) {
+        const int s = c % S, use = c / S;
+        if (!ts_mbar_wait(&pp->full[s], use & 1, TS_TC_WAIT_LIMIT)) {
+          ts_tc_flag(pp);
+          break;
+        }
+        ts_tc_fence_after();
+        const unsigned ahi = ts_smem_u32(smem + s * stage), alo = ahi + 16384;
+        const unsigned bhi = ahi + 2 * 16384, blo = bhi + bbytes;
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+          const unsigned acc = (c > 0 || kk > 0) ? 1u : 0u;
+          ts_mma_tf32(tmem, ts_umma_desc(ahi + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, acc);
+          ts_mma_tf32(tmem, ts_umma_desc(ahi + kk * 32), ts_umma_desc(blo + kk * 32), idesc, 1u);
+          ts_mma_tf32(tmem, ts_umma_desc(alo + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, 1u);
+        }
+        ts_mma_commit(&pp->empty[s]);
+      }
+      ts_mma_commit(&pp->done);
     }
   }
-  if (ok && C > 0) ok = ts_mbar_wait(&bars[(C - 1) & 1], ((C - 1) >> 1) & 1, TS_TC_WAIT_LIMIT);
-  ok = __syncthreads_and(ok);
-  ts_tc_fence_after();
-  if (ok) {
-    // TMEM -> shared [j][comp][field], then the epilogue per (lm, comp)
-    float *sD = reinterpret_cast<float *>(smem);
-    const int row = warp * 32 + lane, fl = row >> 1, comp = row & 1;
-    for (int c0 = 0; c0 < N; c0 += 16) {
-      float v[16];
-      ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
+
+  // ---- epilogue: TMEM -> shared [j][comp][field] -> Epi per (lm, comp)
+  bool ok = true;
+  if (warp < 4) {
+    ok = ts_mbar_wait(&pp->done, 0, TS_TC_WAIT_LIMIT) && !pp->bad;
+    ts_tc_fence_after();
+    if (ok) {
+      float *sD = reinterpret_cast<float *>(smem);
+      const int row = warp * 32 + lane, fl = row >> 1, comp = row & 1;
+      for (int c0 = 0; c0 < N; c0 += 16) {
+        float v[16];
+        ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
 #pragma unroll
-      for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_FIELDS + fl] = v[i];
+        for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_FIELDS + fl] = v[i];
+      }
     }
-    ts_tc_fence_before();
-    __syncthreads();
+  }
+  ts_tc_fence_before();
+  ok = __syncthreads_and(ok || warp >= 4) && !pp->bad;
+  if (ok) {
+    const float *sD = reinterpret_cast<const float *>(smem);
     for (int idx = tid; idx < cnt * 2; idx += blockDim.x) {
       const int j = idx >> 1, cp = idx & 1;
       const int l = m + par + 2 * (ltile * tc.LTL + j);

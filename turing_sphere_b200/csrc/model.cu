@@ -668,9 +668,10 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
         int per_cta = s.per_cta;
         if (p->precision != TS_PREC_FP32) {
           TsTcTab tc = ts_tc_tab(p);
-          void *args[] = {&leg, &tc, &g, &gs, &epi, &nfields, &per_cta};
+          int S = ts_tc_analys_stages(p);
+          void *args[] = {&leg, &tc, &g, &gs, &epi, &nfields, &per_cta, &S};
           dim3 grid((nfields + per_cta - 1) / per_cta, p->mmax + 1, 2 * ts_tc_ntile(p));
-          TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(128), args, s.smem, st));
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(192), args, s.smem, st));
         } else {
           void *args[] = {&leg, &g, &gs, &epi, &nfields, &per_cta};
           dim3 grid(p->mmax + 1, (nfields + per_cta - 1) / per_cta);

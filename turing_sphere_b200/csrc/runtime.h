@@ -109,6 +109,8 @@ int ts_tc_ntile(ts_plan p);
 size_t ts_tc_bytes(ts_plan p);
 size_t ts_tc_synth_smem(ts_plan p);
 size_t ts_tc_analys_smem(ts_plan p);
+int ts_tc_synth_stages(ts_plan p);
+int ts_tc_analys_stages(ts_plan p);
 void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fm_stride, int nfields,
                             cudaStream_t s);
 void ts_launch_leg_analys_tc(ts_plan p, const float2 *g, long g_stride, float2 *q, long q_stride,

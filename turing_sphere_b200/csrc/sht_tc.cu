@@ -171,16 +171,33 @@ const TsTcTab &ts_tc_tab(ts_plan p) { return static_cast<ts_tc_tables *>(p->tc)-
 int ts_tc_ntile(ts_plan p) { return static_cast<ts_tc_tables *>(p->tc)->ntile; }
 size_t ts_tc_bytes(ts_plan p) { return p->tc ? static_cast<ts_tc_tables *>(p->tc)->bytes : 0; }
 
+// pipeline depth and shared memory of the two kernels
+namespace {
+const size_t kSmemBudget = 227 * 1024 - 2048;
+int synth_stages(ts_plan p) {
+  const size_t stage = 2 * 16384 + 2 * (size_t)ts_tc_tab(p).NL * 128;
+  return (int)std::min<size_t>(TS_TC_MAXSTAGE, kSmemBudget / stage);
+}
+int analys_N(ts_plan p) { return std::min(256, ((kpar_h(p->lmax, 0, 0) + 15) / 16) * 16); }
+}  // namespace
+
+int ts_tc_synth_stages(ts_plan p) { return synth_stages(p); }
+int ts_tc_analys_stages(ts_plan p) {
+  // the planner's dry run has no tables: derive from the grid alone
+  const size_t stage = 2 * 16384 + 2 * (size_t)analys_N(p) * 128;
+  return (int)std::min<size_t>(TS_TC_MAXSTAGE, kSmemBudget / stage);
+}
+
 size_t ts_tc_synth_smem(ts_plan p) {
-  const int NL = ts_tc_tab(p).NL;
-  const size_t stage = 2 * (size_t)NL * 128 + 2 * 16384;
-  return std::max(2 * stage, (size_t)2 * TS_TC_ROWS * (NL + 1) * 4) + 1024 + 64;
+  const size_t stage = 2 * 16384 + 2 * (size_t)ts_tc_tab(p).NL * 128;
+  return synth_stages(p) * stage + 1024 + sizeof(TsTcPipe);
 }
 
 size_t ts_tc_analys_smem(ts_plan p) {
-  const int N = std::min(256, ((kpar_h(p->lmax, 0, 0) + 15) / 16) * 16);
+  const int N = analys_N(p);
   const size_t stage = 2 * 16384 + 2 * (size_t)N * 128;
-  return std::max(2 * stage, (size_t)N * 2 * TS_TC_FIELDS * 4) + 1024 + 64;
+  return std::max(ts_tc_analys_stages(p) * stage, (size_t)N * 2 * TS_TC_FIELDS * 4) + 1024 +
+         sizeof(TsTcPipe);
 }
 
 void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fs, int nf,
@@ -193,7 +210,8 @@ void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fs, i
   }
   const TsTcTab &tc = ts_tc_tab(p);
   dim3 grid((nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS, p->mmax + 1, tc.nLT);
-  ts_leg_synth_tc<<<grid, 128, ts_tc_synth_smem(p), s>>>(p->leg, tc, q, fm, fs, nf);
+  ts_leg_synth_tc<<<grid, TS_TC_THREADS, ts_tc_synth_smem(p), s>>>(p->leg, tc, q, fm, fs, nf,
+                                                                    synth_stages(p));
   TS_CUDA(cudaGetLastError());
 }
 
@@ -209,8 +227,8 @@ void ts_launch_leg_analys_tc(ts_plan p, const float2 *g, long gs, float2 *out, l
   const TsTcTab &tc = ts_tc_tab(p);
   dim3 grid((nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS, p->mmax + 1, 2 * ts_tc_ntile(p));
   TsAnalysStore epi{out, os};
-  ts_leg_analys_tc<TsAnalysStore><<<grid, 128, ts_tc_analys_smem(p), s>>>(p->leg, tc, g, gs, epi,
-                                                                          nf, TS_TC_FIELDS);
+  ts_leg_analys_tc<TsAnalysStore><<<grid, TS_TC_THREADS, ts_tc_analys_smem(p), s>>>(
+      p->leg, tc, g, gs, epi, nf, TS_TC_FIELDS, ts_tc_analys_stages(p));
   TS_CUDA(cudaGetLastError());
 }
 
