@@ -56,7 +56,7 @@ struct Stage {
   cudaKernel_t kern = nullptr;
   std::vector<Ref> in, out;
   int nsyn = 0, nana = 0;
-  int lb = 0, F = 1, K = 1, W = 1, per_cta = 1;
+  int lb = 0, F = 1, K = 1, W = 1, per_cta = 1, r1 = 0;
   size_t smem = 0;
   std::string label;  // one line, for describe()
   std::string src;    // generated CUDA of this stage
@@ -411,7 +411,10 @@ void schedule(ts_model m, Program &P, bool is_step) {
       for (size_t o = 0; o < gout.size(); o++)
         src << "    out[" << A.size() + o << "] = " << em.name.at(gout[o]) << ";\n";
       src << "  }\n};\n";
-      st.expr = "ts_fourier_phase<" + pn + ">";
+      const int r1 = ts_fft_r1(p);
+      st.expr = r1 ? "ts_fourier_phase_r<" + pn + ", " + std::to_string(r1) + ">"
+                   : "ts_fourier_phase<" + pn + ">";
+      st.r1 = r1;
       st.label = "phase   " + std::to_string(S.size()) + " synth, " + std::to_string(G.size()) +
                  " grid statement(s), " + std::to_string(A.size()) + " analys";
       st.src = src.str();
@@ -701,7 +704,7 @@ void finish_shapes(ts_model m) {
     for (auto &s : P.stages) {
       if (s.kind == Stage::Phase) {
         const int nrows = s.nsyn + s.nana + 1;
-        s.lb = ts_fourier_lb(p, m->batch, nrows, &s.smem);
+        s.lb = s.r1 ? ts_rfft_lb(p, m->batch, 1, &s.smem) : ts_fourier_lb(p, m->batch, nrows, &s.smem);
       } else if (s.kind == Stage::LegAnalys) {
         s.smem = p->precision != TS_PREC_FP32 ? ts_tc_analys_smem(p) : ts_analys_smem(p, s.F, s.W);
       }

@@ -99,6 +99,9 @@ void ts_analys_shape(ts_plan p, int nfields, int per_inst, int *F, int *K, int *
 size_t ts_analys_smem(ts_plan p, int F, int W);
 // rows per Fourier CTA for a kernel holding `nrows` rows per warp
 int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem);
+// warp-register FFT: R1 = H/32 (0 = not applicable) and rows per CTA
+int ts_fft_r1(ts_plan p);
+int ts_rfft_lb(ts_plan p, int nblocks_y, int nrowbuf, size_t *smem);
 void ts_init_tables(ts_plan p);
 // tensor-core tables and kernels (sht_tc.cu)
 struct TsTcTab;

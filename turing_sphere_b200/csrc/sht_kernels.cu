@@ -364,8 +364,79 @@ void ts_launch_leg_analys(ts_plan p, const float2 *g, long gs, float2 *q, long q
   return leg_analys_f<1>(p, K, W, g, gs, q, qs, nf, s);
 }
 
+// R1 of the warp-register FFT (H = 32 R1), 0 when the row does not fit it
+int ts_fft_r1(ts_plan p) {
+  if (p->fourier != TS_FOURIER_FFT) return 0;
+  const int H = p->fft.H;
+  if (H % 32) return 0;
+  const int r1 = H / 32;
+  switch (r1) {
+    case 1: case 2: case 3: case 4: case 6: case 8: case 12: case 16: case 24: return r1;
+    default: return 0;
+  }
+}
+
+// rows per register-FFT CTA: enough CTAs to fill the GPU twice, <= 8
+int ts_rfft_lb(ts_plan p, int nblocks_y, int nrowbuf, size_t *smem) {
+  int lb = 8;
+  for (; lb > 1; lb >>= 1) {
+    const long ctas = (long)nblocks_y * ((p->nlat + lb - 1) / lb);
+    if (ctas >= 2L * p->ctx->sm_count) break;
+  }
+  *smem = sizeof(float2) * ((size_t)p->nphi + p->fft.H + (size_t)lb * (p->mmax + 2) +
+                            (size_t)lb * nrowbuf * p->fft.H);
+  TS_REQUIRE(*smem <= p->ctx->smem_optin, TS_ERR_UNSUPPORTED, "grid too large for the register FFT");
+  return lb;
+}
+
+namespace {
+template <int R1>
+void rsynth(ts_plan p, const float2 *fm, long fs, float *spat, long ss, int nf, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    TS_CUDA(cudaFuncSetAttribute(ts_fourier_synth_r<R1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)p->ctx->smem_optin));
+    attr = true;
+  }
+  size_t smem;
+  const int lb = ts_rfft_lb(p, nf, 1, &smem);
+  dim3 grid((p->nlat + lb - 1) / lb, nf);
+  ts_fourier_synth_r<R1><<<grid, 32 * lb, smem, s>>>(p->fft, fm, fs, spat, ss);
+  TS_CUDA(cudaGetLastError());
+}
+template <int R1>
+void ranalys(ts_plan p, const float *spat, long ss, float2 *g, long gs, int nf, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    TS_CUDA(cudaFuncSetAttribute(ts_fourier_analys_r<R1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)p->ctx->smem_optin));
+    attr = true;
+  }
+  size_t smem;
+  const int lb = ts_rfft_lb(p, nf, 1, &smem);
+  dim3 grid((p->nlat + lb - 1) / lb, nf);
+  ts_fourier_analys_r<R1><<<grid, 32 * lb, smem, s>>>(p->fft, spat, ss, g, gs);
+  TS_CUDA(cudaGetLastError());
+}
+#define TS_R1_SWITCH(r1, F, ...)          \
+  switch (r1) {                           \
+    case 1: return F<1>(__VA_ARGS__);     \
+    case 2: return F<2>(__VA_ARGS__);     \
+    case 3: return F<3>(__VA_ARGS__);     \
+    case 4: return F<4>(__VA_ARGS__);     \
+    case 6: return F<6>(__VA_ARGS__);     \
+    case 8: return F<8>(__VA_ARGS__);     \
+    case 12: return F<12>(__VA_ARGS__);   \
+    case 16: return F<16>(__VA_ARGS__);   \
+    case 24: return F<24>(__VA_ARGS__);   \
+  }
+}  // namespace
+
 void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, long ss, int nf,
                              cudaStream_t s) {
+  if (const int r1 = ts_fft_r1(p)) {
+    TS_R1_SWITCH(r1, rsynth, p, fm, fs, spat, ss, nf, s)
+  }
   if (p->fourier == TS_FOURIER_DFT) {
     dim3 grid((p->nphi + 63) / 64, p->nlat, nf);
     ts_k_dft_synth<<<grid, 64, 0, s>>>(p->fft, fm, fs, spat, ss);
@@ -381,6 +452,9 @@ void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, 
 
 void ts_launch_fourier_analys(ts_plan p, const float *spat, long ss, float2 *g, long gs, int nf,
                               cudaStream_t s) {
+  if (const int r1 = ts_fft_r1(p)) {
+    TS_R1_SWITCH(r1, ranalys, p, spat, ss, g, gs, nf, s)
+  }
   if (p->fourier == TS_FOURIER_DFT) {
     dim3 grid((p->mmax + 1 + 63) / 64, p->nlat, nf);
     ts_k_dft_analys<<<grid, 64, 0, s>>>(p->fft, spat, ss, g, gs);
