@@ -130,7 +130,9 @@ int ts_sht_analys_dev(ts_plan plan, const float *spat, float *qlm, int batch, vo
  * exceeds 16 MiB ((mmax+1)*nlat*8 bytes per field) fails with TS_ERR_SIZE.
  * The first call on a device looks up the array's device address; make that
  * first call before any stream capture.  All calls share the one array: calls
- * that overlap on the GPU (different streams, no ordering) race. */
+ * that overlap on the GPU (different streams, no ordering) race.  It runs the
+ * FP32 Legendre kernels whatever the plan's precision (the tensor-core path
+ * needs an operand image the plan grows on demand). */
 int ts_sht_synth_noalloc(ts_plan plan, const float *qlm, float *spat, int batch, void *stream);
 
 /* Blocking transforms on host arrays (ShtPlan.synth / ShtPlan.analys,

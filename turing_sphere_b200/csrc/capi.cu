@@ -104,6 +104,7 @@ void synth_dev(ts_plan p, const float *qlm, float *spat, int batch, cudaStream_t
 }
 
 void analys_dev(ts_plan p, const float *spat, float *qlm, int batch, cudaStream_t s) {
+  if (p->precision != TS_PREC_FP32) return ts_analys_tc_full(p, spat, npts_of(p), qlm, batch, s);
   const long fm_stride = (long)(p->mmax + 1) * p->nlat;
   p->fm.ensure(sizeof(float2) * fm_stride * batch);
   float2 *fm = (float2 *)p->fm.p;

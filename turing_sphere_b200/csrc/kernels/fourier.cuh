@@ -684,3 +684,202 @@ __global__ void __launch_bounds__(256) ts_fourier_phase_r(TsFftTab ft, TsPhaseIO
     __syncthreads();
   }
 }
+
+// ------------------------------------------ analysis into the TC operand image
+//
+// Tensor-core plans consume the analysis as W_par = w (G_north +- G_south)
+// in the MMA's byte image (TsTcImg.w).  A CTA therefore takes NP northern
+// latitudes and their southern mirrors (warp w: rows lat0+w and
+// nlat-1-lat0-w) and writes the folded, weighted values straight into the
+// image: 32-byte runs of 8 latitudes per (m, parity, re|im).
+TS_DEV void ts_write_wimg(const float2 *tN, const float2 *tS, int P, int NP, int lat0, long f,
+                          const TsFftTab &ft, const float *wq, char *wimg, int nfb, int fpb,
+                          int nlc, int nh) {
+  const long fb = f / fpb;
+  const int fl = (int)(f - fb * fpb);
+  const int n = (ft.mmax + 1) * 4 * NP;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    const int w = idx % NP;
+    const int rest = idx / NP;
+    const int comp = rest & 1, par = (rest >> 1) & 1, m = rest >> 2;
+    const int lat = lat0 + w;
+    if (lat >= nh) continue;
+    const float2 xn = tN[w * P + m], xs = tS[w * P + m];
+    const float a = comp ? xn.y : xn.x, b = comp ? xs.y : xs.x;
+    const float v = wq[lat] * (par ? a - b : a + b);
+    const long blk = (((long)m * nfb + fb) * 2 + par) * nlc + (lat >> 5);
+    *reinterpret_cast<float *>(wimg + blk * 16384 + ts_swz_img(2 * fl + comp, lat & 31)) = v;
+  }
+}
+
+// spat[field][lat][phi] -> W image.  grid = (ceil(nh/NP), nfields), block = 32*NP.
+// Shared memory: tw[nphi] | twr[H] | tileN[NP][P] | tileS[NP][P] | rowbuf[NP][H].
+template <int R1>
+__global__ void __launch_bounds__(256)
+ts_fourier_analys_rw(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
+                     const float *__restrict__ wq, char *wimg, int nfb, int fpb, int nlc, int nh) {
+  extern __shared__ float2 ts_smem_rw[];
+  const int NP = blockDim.x >> 5;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lat0 = blockIdx.x * NP;
+  const long f = blockIdx.y;
+  const int P = ts_rtile_pitch(ft);
+  float2 *stw = ts_smem_rw;
+  float2 *twr = stw + ft.nphi;
+  float2 *tN = twr + ft.H;
+  float2 *tS = tN + NP * P;
+  float2 *rowbuf = tS + NP * P + (long)w * ft.H;
+  ts_load_tw(stw, ft);
+  __syncthreads();
+  ts_load_twr(twr, stw, R1, ft.nphi);
+  __syncthreads();
+  const int latN = lat0 + w;
+  if (latN < nh) {
+    float2 w5[5];
+    ts_lane_twiddles(w5, stw, ft.nphi, lane);
+    const int latS = ft.nlat - 1 - latN;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      float2 *trow = (h ? tS : tN) + w * P;
+      if (h && latS == latN) {  // the equator counts once
+        for (int k = lane; k <= ft.mmax; k += 32) trow[k] = make_float2(0.f, 0.f);
+        continue;
+      }
+      const float2 *in = reinterpret_cast<const float2 *>(spat + f * spat_stride +
+                                                          (long)(h ? latS : latN) * ft.nphi);
+      float2 x[R1];
+#pragma unroll
+      for (int j = 0; j < R1; j++) x[j] = in[lane + 32 * j];
+      ts_fft_dif<R1, -1>(x, stw, twr, w5, ft.nphi, lane);
+      __syncwarp();
+#pragma unroll
+      for (int k1 = 0; k1 < R1; k1++) rowbuf[k1 + R1 * ts_rev5(lane)] = x[k1];
+      __syncwarp();
+      ts_runpack(rowbuf, trow, stw, ft, lane);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  ts_write_wimg(tN, tS, P, NP, lat0, f, ft, wq, wimg, nfb, fpb, nlc, nh);
+}
+
+// stage fm[m][lat] of northern (h = 0) or mirrored southern (h = 1) rows of
+// the CTA's latitude pairs into tile[w][k]
+TS_DEV void ts_load_rtile_pairs(float2 *tile, const float2 *src, int lat0, int NP, int h,
+                                int nh, const TsFftTab &ft) {
+  const int P = ts_rtile_pitch(ft);
+  const int n = (ft.mmax + 1) * NP;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    const int k = idx / NP, w = idx - k * NP;
+    const int latN = lat0 + w;
+    const int lat = h ? ft.nlat - 1 - latN : latN;
+    tile[w * P + k] = latN < nh ? src[(long)k * ft.nlat + lat] : make_float2(0.f, 0.f);
+  }
+}
+
+// Fused model phase for tensor-core plans: as ts_fourier_phase_r, but over
+// north/south latitude pairs, with the analysis outputs written as the W image
+// the tensor-core analysis reads.  grid = (ceil(nh/NP), instances), block =
+// 32*NP.  Shared memory: tw | twr | tin[NP][P] | tout[2][NANA][NP][P] |
+// rowbuf[NP][H].
+template <class Prog, int R1>
+__global__ void __launch_bounds__(256) ts_fourier_phase_rw(TsFftTab ft, TsPhaseIO io) {
+  constexpr int NSYN = Prog::NSYN, NGIN = Prog::NGIN, NANA = Prog::NANA, NGOUT = Prog::NGOUT;
+  constexpr int NIN = NSYN + NGIN > 0 ? NSYN + NGIN : 1;
+  constexpr int NOUT = NANA + NGOUT > 0 ? NANA + NGOUT : 1;
+  constexpr int NA = NANA > 0 ? NANA : 1;
+  extern __shared__ float2 ts_smem_rpw[];
+  const int NP = blockDim.x >> 5;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lat0 = blockIdx.x * NP;
+  const long inst = blockIdx.y;
+  const int P = ts_rtile_pitch(ft);
+  float2 *stw = ts_smem_rpw;
+  float2 *twr = stw + ft.nphi;
+  float2 *tin = twr + ft.H;
+  float2 *tout = tin + NP * P;  // [h][k][w][P]
+  float2 *rowbuf = tout + 2 * NA * NP * P + (long)w * ft.H;
+  ts_load_tw(stw, ft);
+  __syncthreads();
+  ts_load_twr(twr, stw, R1, ft.nphi);
+  __syncthreads();
+  float2 w5[5];
+  ts_lane_twiddles(w5, stw, ft.nphi, lane);
+  const int latN = lat0 + w;
+  const float *prm = io.prm + inst * io.nprm;
+
+#pragma unroll 1
+  for (int h = 0; h < 2; h++) {
+    const int lat = h ? ft.nlat - 1 - latN : latN;
+    const bool equator_south = h && lat == latN;
+    const bool live = latN < io.nh && !equator_south;
+    const long rowoff = (long)lat * ft.nphi;
+    float2 v[NIN][R1];
+#pragma unroll
+    for (int s = 0; s < NSYN; s++) {
+      __syncthreads();
+      ts_load_rtile_pairs(tin, io.fm + (inst * NSYN + s) * io.field, lat0, NP, h, io.nh, ft);
+      __syncthreads();
+      if (live) {
+        ts_rpack<R1>(v[s], tin + w * P, stw, ft, lane);
+        ts_fft_dif<R1, +1>(v[s], stw, twr, w5, ft.nphi, lane);
+      }
+    }
+#pragma unroll
+    for (int gi = 0; gi < NGIN; gi++) {
+      if (live) {
+        const float2 *src = reinterpret_cast<const float2 *>(io.gin[gi] + inst * io.gin_stride[gi] + rowoff);
+        __syncwarp();
+        for (int n = lane; n < ft.H; n += 32) rowbuf[n] = src[n];
+        __syncwarp();
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) v[NSYN + gi][k1] = rowbuf[k1 + R1 * ts_rev5(lane)];
+      }
+    }
+    float2 r[NOUT][R1];
+    if (live) {
+#pragma unroll
+      for (int k1 = 0; k1 < R1; k1++) {
+        float in0[NIN], in1[NIN], o0[NOUT], o1[NOUT];
+#pragma unroll
+        for (int i = 0; i < NSYN + NGIN; i++) {
+          in0[i] = v[i][k1].x;
+          in1[i] = v[i][k1].y;
+        }
+        Prog::eval(in0, o0, prm);
+        Prog::eval(in1, o1, prm);
+#pragma unroll
+        for (int o = 0; o < NANA + NGOUT; o++) r[o][k1] = make_float2(o0[o], o1[o]);
+      }
+#pragma unroll
+      for (int o = 0; o < NGOUT; o++) {
+        __syncwarp();
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) rowbuf[k1 + R1 * ts_rev5(lane)] = r[NANA + o][k1];
+        __syncwarp();
+        float2 *dst = reinterpret_cast<float2 *>(io.gout[o] + inst * io.gout_stride[o] + rowoff);
+        for (int n = lane; n < ft.H; n += 32) dst[n] = rowbuf[n];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NANA; k++) {
+      float2 *trow = tout + ((long)(h * NA + k) * NP + w) * P;
+      if (live) {
+        ts_fft_dit<R1, -1>(r[k], stw, twr, w5, ft.nphi, lane);
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < R1; j++) rowbuf[lane + 32 * j] = r[k][j];
+        __syncwarp();
+        ts_runpack(rowbuf, trow, stw, ft, lane);
+        __syncwarp();
+      } else if (equator_south) {
+        for (int kk = lane; kk <= ft.mmax; kk += 32) trow[kk] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NANA; k++)
+    ts_write_wimg(tout + (long)k * NP * P, tout + (long)(NA + k) * NP * P, P, NP, lat0,
+                  inst * NANA + k, ft, io.wq, io.wimg, io.w_nfb, io.w_fpb, io.w_nlc, io.nh);
+}

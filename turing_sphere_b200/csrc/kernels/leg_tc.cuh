@@ -12,12 +12,19 @@
 // data operand (Q or W) is split on the fly: hi = rna_tf32(x),
 // lo = rna_tf32(x - hi); each k-step issues hi*hi + hi*lo + lo*hi.
 //
-// Warp roles (192 threads): warps 0-3 build the data operand of each stage
-// and run the epilogue (they own TMEM lanes 0-127), warp 4 streams the table
-// chunks with cp.async.bulk (expect-tx mbarrier), warp 5 issues the MMAs and
-// commits each stage back to its producers.  Every wait is bounded: on
-// timeout the kernel records an error flag, skips the epilogue, frees its
-// tensor memory and returns.
+// Both operands reach shared memory by cp.async.bulk: the P table from its
+// precomputed image and the data operand from a raw-fp32 image of the same
+// byte layout (TsTcImg; written by a relayout kernel for the synthesis and by
+// the Fourier analysis itself for the analysis).  The kernels are persistent
+// (one CTA per SM walking tiles blockIdx.x + k*gridDim.x) with 320 threads in
+// fixed roles: warps 0-3 split each data tile in place into rna-rounded TF32
+// hi and lo, warp 4 issues the copies (expect-tx mbarriers over an S-slot
+// ring), warp 5 issues the MMAs, warps 6-9 drain the accumulators.  Tensor
+// memory holds two accumulator buffers, so the epilogue of tile i overlaps the
+// MMAs of tile i+1 and the operand ring streams across tile boundaries.
+// Every wait is bounded: on timeout the kernel records an error flag, waits
+// (bounded) for its copies and MMAs in flight, frees its tensor memory and
+// returns.
 #pragma once
 #include "ts_common.cuh"
 
@@ -174,6 +181,45 @@ TS_DEV long ts_atile_offset(const TsTcTab &tc, int lmax, int m, int par, int lti
   return off;
 }
 
+#define TS_TC_THREADS 320
+#define TS_TC_MAXSTAGE 4
+
+// Persistent pipeline state.  Operand ring: full[s] the copies of slot s
+// landed; ready[s] the 4 split warps converted its data tile; empty[s] the
+// MMAs that read it are done.  Accumulators (two TMEM buffers): acc_full[b]
+// the MMAs of a tile into buffer b are done; acc_empty[b] the epilogue warps
+// have read it out.
+struct TsTcPipe {
+  unsigned long long full[TS_TC_MAXSTAGE], ready[TS_TC_MAXSTAGE], empty[TS_TC_MAXSTAGE];
+  unsigned long long acc_full[2], acc_empty[2];
+  unsigned long long epi;    // the 4 epilogue warps' own barrier
+  unsigned long long drain;  // the MMA warp's last commit before exit
+  unsigned tmem;
+  int bad;
+};
+
+TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S) {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; s++) {
+      ts_mbar_init(&pp->full[s], 1);
+      ts_mbar_init(&pp->ready[s], 4);
+      ts_mbar_init(&pp->empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      ts_mbar_init(&pp->acc_full[b], 1);
+      ts_mbar_init(&pp->acc_empty[b], 4);
+    }
+    ts_mbar_init(&pp->epi, 4);
+    ts_mbar_init(&pp->drain, 1);
+    pp->bad = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+}
+
+TS_DEV bool ts_tc_bad(const TsTcPipe *pp) { return *reinterpret_cast<const volatile int *>(&pp->bad); }
+
+TS_DEV void ts_tc_flag(TsTcPipe *pp) { atomicExch(&pp->bad, 1); }
+
 TS_DEV void ts_mbar_arrive(unsigned long long *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(ts_smem_u32(bar)) : "memory");
 }
@@ -193,353 +239,392 @@ TS_DEV void ts_bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned lon
       : "memory");
 }
 
-#define TS_TC_THREADS 192
-#define TS_TC_MAXSTAGE 4
-
-// Pipeline bookkeeping shared by both kernels: full[s] completes when the
-// table bytes of stage s have landed and the 4 producer warps have arrived;
-// empty[s] completes when the MMAs that read stage s are done; done[0] when
-// all MMAs are.
-struct TsTcPipe {
-  unsigned long long full[TS_TC_MAXSTAGE], empty[TS_TC_MAXSTAGE], done;
-  unsigned tmem;
-  int bad;
-};
-
-TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S) {
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < S; s++) {
-      ts_mbar_init(&pp->full[s], 5);
-      ts_mbar_init(&pp->empty[s], 1);
-    }
-    ts_mbar_init(&pp->done, 1);
-    pp->bad = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+// warps 0-3: split the raw fp32 tile at `ahi` in place into hi = rna_tf32(x)
+// and lo = rna_tf32(x - hi) at `alo` (element order is irrelevant: it is a
+// pure element-wise map over the 16 KB block)
+TS_DEV void ts_tc_split16k(char *ahi, char *alo, int tid) {
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int off = (tid + i * 128) * 16;
+    const float4 x = *reinterpret_cast<const float4 *>(ahi + off);
+    float4 h, l;
+    h.x = ts_rna_tf32(x.x);
+    h.y = ts_rna_tf32(x.y);
+    h.z = ts_rna_tf32(x.z);
+    h.w = ts_rna_tf32(x.w);
+    l.x = ts_rna_tf32(x.x - h.x);
+    l.y = ts_rna_tf32(x.y - h.y);
+    l.z = ts_rna_tf32(x.z - h.z);
+    l.w = ts_rna_tf32(x.w - h.w);
+    *reinterpret_cast<float4 *>(ahi + off) = h;
+    *reinterpret_cast<float4 *>(alo + off) = l;
   }
 }
 
-TS_DEV void ts_tc_flag(TsTcPipe *pp) { atomicExch(&pp->bad, 1); }
+// MMA issue (one thread): per tile, wait until the epilogue has drained the
+// accumulator buffer, then per stage wait for the split data tile, issue the
+// 3-pass products of its 4 k-steps and commit the slot back to the copy warp;
+// the tile's last commit signals the epilogue.
+template <class Sched>
+TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes, unsigned tmem,
+                           int acc_cols, const Sched &sc) {
+  const int ntiles = sc.ntiles();
+  long g = 0;
+  int i = 0;
+  for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x, i++) {
+    const int b = i & 1;
+    if (i >= 2 && !ts_mbar_wait(&pp->acc_empty[b], ((i >> 1) - 1) & 1, TS_TC_WAIT_LIMIT)) {
+      ts_tc_flag(pp);
+      return;
+    }
+    ts_tc_fence_after();
+    const int T = sc.stages(tile);
+    const unsigned tb = sc.table_bytes(tile);
+    const unsigned idesc = ts_idesc_tf32(sc.n(tile));
+    for (int t_ = 0; t_ < T; t_++, g++) {
+      const int s = (int)(g % S);
+      const unsigned use = (unsigned)(g / S);
+      if (!ts_mbar_wait(&pp->ready[s], use & 1, TS_TC_WAIT_LIMIT)) {
+        ts_tc_flag(pp);
+        return;
+      }
+      ts_tc_fence_after();
+      const unsigned ahi = ts_smem_u32(smem + s * stage_bytes), alo = ahi + 16384;
+      const unsigned bhi = ahi + 2 * 16384, blo = bhi + tb / 2;
+      const unsigned d = tmem + (unsigned)(b * acc_cols + sc.d_col(tile, t_));
+      const bool init = sc.first(tile, t_);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const unsigned acc = (!init || kk > 0) ? 1u : 0u;
+        ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, acc);
+        ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(blo + kk * 32), idesc, 1u);
+        ts_mma_tf32(d, ts_umma_desc(alo + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, 1u);
+      }
+      ts_mma_commit(&pp->empty[s]);
+    }
+    ts_mma_commit(&pp->acc_full[b]);
+  }
+}
+
+// Persistent schedule.  The CTA takes tiles blockIdx.x, blockIdx.x +
+// gridDim.x, ...; `Sched` maps a tile to its stage count and, per stage, the
+// data tile, the table chunk and the accumulator column; every role walks the
+// same sequence, so ring slots and barrier phases stay in step.  Warps 0-3
+// split data tiles, warp 4 copies, warp 5 issues MMAs, warps 6-9 drain the
+// accumulators through `epilogue(tile, tmem_cols_of_buffer)`.
+template <class Sched, class Epilogue>
+TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes, unsigned tmem,
+                             int acc_cols, const Sched &sc, Epilogue epilogue) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntiles = sc.ntiles();
+  if (warp < 4) {
+    long g = 0;
+    for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x) {
+      const int T = sc.stages(tile);
+      for (int t_ = 0; t_ < T; t_++, g++) {
+        const int s = (int)(g % S);
+        const unsigned use = (unsigned)(g / S);
+        if (!ts_mbar_wait(&pp->full[s], use & 1, TS_TC_WAIT_LIMIT)) {
+          ts_tc_flag(pp);
+          return;
+        }
+        char *ahi = smem + s * stage_bytes;
+        ts_tc_split16k(ahi, ahi + 16384, tid);
+        ts_fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) ts_mbar_arrive(&pp->ready[s]);
+      }
+    }
+  } else if (warp == 4) {
+    if (lane == 0) {
+      long g = 0;
+      for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x) {
+        const int T = sc.stages(tile);
+        const unsigned tb = sc.table_bytes(tile);
+        int t_ = 0;
+        for (; t_ < T; t_++, g++) {
+          const int s = (int)(g % S);
+          const unsigned use = (unsigned)(g / S);
+          if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
+            ts_tc_flag(pp);
+            break;
+          }
+          char *st = smem + s * stage_bytes;
+          ts_mbar_arrive_tx(&pp->full[s], 16384 + tb);
+          ts_bulk_g2s(st, sc.a_src(tile, t_), 16384, &pp->full[s]);
+          ts_bulk_g2s(st + 2 * 16384, sc.b_src(tile, t_), tb, &pp->full[s]);
+        }
+        if (t_ < T) break;
+      }
+      // no copy may still be landing in shared memory when the CTA exits:
+      // wait (bounded) for the last use of every slot that was issued
+      for (int s = 0; s < S && s < g; s++) {
+        const unsigned last = (unsigned)((g - 1 - s) / S);
+        if (!ts_mbar_wait(&pp->full[s], last & 1, TS_TC_WAIT_LIMIT)) ts_tc_flag(pp);
+      }
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      ts_tc_mma_role(smem, pp, S, stage_bytes, tmem, acc_cols, sc);
+      // every MMA this thread issued has finished before TMEM is released
+      ts_mma_commit(&pp->drain);
+      if (!ts_mbar_wait(&pp->drain, 0, TS_TC_WAIT_LIMIT)) ts_tc_flag(pp);
+    }
+  } else {
+    int i = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
+      const int b = i & 1;
+      const bool ok = ts_mbar_wait(&pp->acc_full[b], (i >> 1) & 1, TS_TC_WAIT_LIMIT);
+      if (!ok || ts_tc_bad(pp)) {
+        ts_tc_flag(pp);
+        return;
+      }
+      ts_tc_fence_after();
+      if (!epilogue(tile, tmem + (unsigned)(b * acc_cols))) {
+        ts_tc_flag(pp);
+        return;
+      }
+      ts_tc_fence_before();
+      __syncwarp();
+      if (lane == 0) ts_mbar_arrive(&pp->acc_empty[b]);
+    }
+  }
+}
+
+// rows 32*(warp%4) .. of TMEM belong to epilogue warp `warp` (warps 6-9)
+TS_DEV int ts_epi_row(int warp, int lane) { return (warp & 3) * 32 + lane; }
+
+// barrier of the 4 epilogue warps, bounded; `phase` counts its uses
+TS_DEV bool ts_epi_sync(TsTcPipe *pp, unsigned &phase) {
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) ts_mbar_arrive(&pp->epi);
+  const bool ok = ts_mbar_wait(&pp->epi, phase & 1, TS_TC_WAIT_LIMIT);
+  phase++;
+  return ok;
+}
 
 // ----------------------------------------------------------------- synthesis
-//
-// grid = (ceil(nfields/64), mmax+1, nLT), block = 192.  Stages (2*16384 bytes
-// of data operand + 2*NL*128 bytes of table each) cycle through the k chunks
-// of both parities, interleaved.  Dynamic shared memory: S*stage + 1024 +
-// sizeof(TsTcPipe).
-__global__ void __launch_bounds__(TS_TC_THREADS, 1)
-ts_leg_synth_tc(TsLegTab t, TsTcTab tc, TsFields q, float2 *__restrict__ fm, long fm_stride,
-                int nfields, int S) {
-  extern __shared__ __align__(1024) char ts_smem_st[];
-  char *smem = (char *)(((unsigned long long)ts_smem_st + 1023) & ~1023ull);
-  const int fb = blockIdx.x, m = blockIdx.y, lt = blockIdx.z;
-  const int NL = tc.NL;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long base = ts_lm_base(t.lmax, m);
-  const int kp0 = ts_kpar(t.lmax, m, 0), kp1 = ts_kpar(t.lmax, m, 1);
-  const int nch0 = (kp0 + TS_TC_KCH - 1) / TS_TC_KCH, nch1 = (kp1 + TS_TC_KCH - 1) / TS_TC_KCH;
-  const int T = nch0 + nch1;
-  const int bbytes = NL * 128;
-  const int stage = 2 * 16384 + 2 * bbytes;  // A hi, A lo, B hi, B lo
-  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage);
-  const unsigned ncols = ts_tmem_cols(2 * NL);
-  // chunk t -> (parity, chunk of that parity): parities interleaved
-  auto chunk = [&](int t_, int &par, int &cc) {
-    const int both = 2 * min(nch0, nch1);
+struct TsSynthSched {
+  const TsTcTab *tc;
+  int lmax, mmax, nfb, NL, nLT;
+  const char *qimg;
+  TS_DEV int ntiles() const { return (mmax + 1) * nLT * nfb; }
+  TS_DEV void decode(int tile, int &m, int &lt, int &fb) const {
+    m = tile / (nLT * nfb);
+    const int r = tile - m * nLT * nfb;
+    lt = r / nfb;
+    fb = r - lt * nfb;
+  }
+  TS_DEV void nch(int m, int &n0, int &n1) const {
+    n0 = (ts_kpar(lmax, m, 0) + TS_TC_KCH - 1) / TS_TC_KCH;
+    n1 = (ts_kpar(lmax, m, 1) + TS_TC_KCH - 1) / TS_TC_KCH;
+  }
+  TS_DEV void parcc(int m, int t_, int &par, int &cc) const {
+    int n0, n1;
+    nch(m, n0, n1);
+    const int both = 2 * min(n0, n1);
     if (t_ < both) {
       par = t_ & 1;
       cc = t_ >> 1;
     } else {
-      par = nch0 > nch1 ? 0 : 1;
-      cc = (t_ - both) + min(nch0, nch1);
+      par = n0 > n1 ? 0 : 1;
+      cc = (t_ - both) + min(n0, n1);
     }
-  };
+  }
+  TS_DEV int stages(int tile) const {
+    int m, lt, fb, n0, n1;
+    decode(tile, m, lt, fb);
+    nch(m, n0, n1);
+    return n0 + n1;
+  }
+  TS_DEV unsigned table_bytes(int) const { return 2u * NL * 128; }
+  TS_DEV int n(int) const { return NL; }
+  TS_DEV const char *a_src(int tile, int t_) const {
+    int m, lt, fb, par, cc, n0, n1;
+    decode(tile, m, lt, fb);
+    parcc(m, t_, par, cc);
+    nch(m, n0, n1);
+    return qimg + ((long)(tc->chunk_prefix[m] + (par ? n0 : 0) + cc) * nfb + fb) * 16384;
+  }
+  TS_DEV const char *b_src(int tile, int t_) const {
+    int m, lt, fb, par, cc, n0, n1;
+    decode(tile, m, lt, fb);
+    parcc(m, t_, par, cc);
+    nch(m, n0, n1);
+    const long bb = 2L * NL * 128;
+    return tc->synth + tc->synth_off[m] + (long)((par ? n0 : 0) + cc) * nLT * bb + (long)lt * bb;
+  }
+  TS_DEV int d_col(int tile, int t_) const {
+    int m, lt, fb, par, cc;
+    decode(tile, m, lt, fb);
+    parcc(m, t_, par, cc);
+    return par * NL;
+  }
+  TS_DEV bool first(int tile, int t_) const {
+    int m, lt, fb, par, cc;
+    decode(tile, m, lt, fb);
+    parcc(m, t_, par, cc);
+    return cc == 0;
+  }
+};
 
+// grid = min(#SMs, tiles), block = 320, persistent.  Dynamic shared memory:
+// S*(2*16384 + 2*NL*128) + 1024 + sizeof(TsTcPipe).  TMEM: two buffers of 2*NL.
+__global__ void __launch_bounds__(TS_TC_THREADS, 1)
+ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb,
+                float2 *__restrict__ fm, long fm_stride, int nfields, int S) {
+  extern __shared__ __align__(1024) char ts_smem_st[];
+  char *smem = (char *)(((unsigned long long)ts_smem_st + 1023) & ~1023ull);
+  const int NL = tc.NL;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned stage = 2 * 16384 + 2 * NL * 128;
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage);
+  const TsSynthSched sc{&tc, t.lmax, t.mmax, q_nfb, NL, tc.nLT, qimg};
   ts_tc_pipe_init(pp, S);
-  if (warp == 0) ts_tmem_alloc(&pp->tmem, ncols);
+  if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
   ts_tc_fence_before();
   __syncthreads();
   ts_tc_fence_after();
   const unsigned tmem = pp->tmem;
 
-  if (warp < 4) {
-    // ---- data operand producers: Q split into TF32 hi/lo, 16 k per thread
-    const int fl = tid & 63, kh = tid >> 6;
-    const int f = fb * TS_TC_FIELDS + fl;
-    const float2 *qf = f < nfields ? ts_field(q, f) + base : nullptr;
-    for (int t_ = 0; t_ < T; t_++) {
-      const int s = t_ % S, use = t_ / S;
-      int par, cc;
-      chunk(t_, par, cc);
-      float2 v[16];
-      const int kp = par ? kp1 : kp0;
-#pragma unroll
-      for (int u = 0; u < 16; u++) {
-        const int j = cc * TS_TC_KCH + kh * 16 + u;
-        v[u] = (qf && j < kp) ? qf[par + 2 * j] : make_float2(0.f, 0.f);
-      }
-      if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
-        ts_tc_flag(pp);
-        break;
-      }
-      char *ahi = smem + s * stage, *alo = ahi + 16384;
-#pragma unroll
-      for (int k4 = 0; k4 < 4; k4++) {
-        const int k = kh * 16 + k4 * 4;
-        float4 h, l;
-        h = make_float4(ts_rna_tf32(v[4 * k4].x), ts_rna_tf32(v[4 * k4 + 1].x),
-                        ts_rna_tf32(v[4 * k4 + 2].x), ts_rna_tf32(v[4 * k4 + 3].x));
-        l = make_float4(ts_rna_tf32(v[4 * k4].x - h.x), ts_rna_tf32(v[4 * k4 + 1].x - h.y),
-                        ts_rna_tf32(v[4 * k4 + 2].x - h.z), ts_rna_tf32(v[4 * k4 + 3].x - h.w));
-        *reinterpret_cast<float4 *>(ahi + ts_swz(2 * fl, k)) = h;
-        *reinterpret_cast<float4 *>(alo + ts_swz(2 * fl, k)) = l;
-        h = make_float4(ts_rna_tf32(v[4 * k4].y), ts_rna_tf32(v[4 * k4 + 1].y),
-                        ts_rna_tf32(v[4 * k4 + 2].y), ts_rna_tf32(v[4 * k4 + 3].y));
-        l = make_float4(ts_rna_tf32(v[4 * k4].y - h.x), ts_rna_tf32(v[4 * k4 + 1].y - h.y),
-                        ts_rna_tf32(v[4 * k4 + 2].y - h.z), ts_rna_tf32(v[4 * k4 + 3].y - h.w));
-        *reinterpret_cast<float4 *>(ahi + ts_swz(2 * fl + 1, k)) = h;
-        *reinterpret_cast<float4 *>(alo + ts_swz(2 * fl + 1, k)) = l;
-      }
-      ts_fence_proxy_async();
-      __syncwarp();
-      if (lane == 0) ts_mbar_arrive(&pp->full[s]);
-    }
-  } else if (warp == 4) {
-    // ---- table stream
-    if (lane == 0) {
-      for (int t_ = 0; t_ < T; t_++) {
-        const int s = t_ % S, use = t_ / S;
-        int par, cc;
-        chunk(t_, par, cc);
-        if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
-          ts_tc_flag(pp);
-          break;
-        }
-        const long src = tc.synth_off[m] + (long)((par ? nch0 : 0) + cc) * tc.nLT * 2 * bbytes +
-                         (long)lt * 2 * bbytes;
-        ts_mbar_arrive_tx(&pp->full[s], 2 * bbytes);
-        ts_bulk_g2s(smem + s * stage + 2 * 16384, tc.synth + src, 2 * bbytes, &pp->full[s]);
-      }
-    }
-  } else {
-    // ---- MMA issue
-    if (lane == 0) {
-      const unsigned idesc = ts_idesc_tf32(NL);
-      for (int t_ = 0; t_ < T; t_++) {
-        const int s = t_ % S, use = t_ / S;
-        int par, cc;
-        chunk(t_, par, cc);
-        if (!ts_mbar_wait(&pp->full[s], use & 1, TS_TC_WAIT_LIMIT)) {
-          ts_tc_flag(pp);
-          break;
-        }
-        ts_tc_fence_after();
-        const unsigned ahi = ts_smem_u32(smem + s * stage), alo = ahi + 16384;
-        const unsigned bhi = ahi + 2 * 16384, blo = bhi + bbytes;
-        const unsigned d = tmem + (unsigned)(par * NL);
-#pragma unroll
-        for (int kk = 0; kk < 4; kk++) {
-          const unsigned acc = (cc > 0 || kk > 0) ? 1u : 0u;
-          ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, acc);
-          ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(blo + kk * 32), idesc, 1u);
-          ts_mma_tf32(d, ts_umma_desc(alo + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, 1u);
-        }
-        ts_mma_commit(&pp->empty[s]);
-      }
-      ts_mma_commit(&pp->done);
-    }
-  }
-
-  // ---- epilogue (warps 0-3 own TMEM lanes 0-127): rows 2f (re) and 2f+1 (im)
-  // sit in adjacent lanes; each pair swaps halves so that every thread writes
-  // 8 consecutive complex values, north and (mirrored) south
-  if (warp < 4) {
-    bool ok = ts_mbar_wait(&pp->done, 0, TS_TC_WAIT_LIMIT) && !pp->bad;
-    ts_tc_fence_after();
-    const int fl = (warp * 32 + lane) >> 1, comp = lane & 1;
+  // epilogue: rows 2f (re) and 2f+1 (im) sit in adjacent lanes; each pair
+  // swaps halves so that every thread writes 8 consecutive complex values,
+  // north and (mirrored) south
+  auto epilogue = [&](int tile, unsigned tbase) -> bool {
+    int m, lt, fb, n0, n1;
+    sc.decode(tile, m, lt, fb);
+    sc.nch(m, n0, n1);
+    const int row = ts_epi_row(warp, lane);
+    const int fl = row >> 1, comp = lane & 1;
     const int f = fb * TS_TC_FIELDS + fl;
     float2 *dst = fm + (long)f * fm_stride + (long)m * t.nlat;
-    if (ok) {
-      for (int c0 = 0; c0 < NL; c0 += 16) {
-        float e[16], o[16];
-        ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, e);
-        if (nch1 > 0)
-          ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(NL + c0), o);
-        else
+    const unsigned lanebase = tbase + ((unsigned)((warp & 3) * 32) << 16);
+    for (int c0 = 0; c0 < NL; c0 += 16) {
+      float e[16], o[16];
+      ts_tmem_ld16(lanebase + (unsigned)c0, e);
+      if (n1 > 0)
+        ts_tmem_ld16(lanebase + (unsigned)(NL + c0), o);
+      else
 #pragma unroll
-          for (int i = 0; i < 16; i++) o[i] = 0.f;
-        // re-lane keeps columns 0-7 and takes the partner's im; im-lane 8-15
-        float2 en[8], on[8];
+        for (int i = 0; i < 16; i++) o[i] = 0.f;
+      float2 en[8], on[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const float se = __shfl_xor_sync(0xffffffffu, comp ? e[i] : e[8 + i], 1);
+        const float so = __shfl_xor_sync(0xffffffffu, comp ? o[i] : o[8 + i], 1);
+        en[i] = comp ? make_float2(se, e[8 + i]) : make_float2(e[i], se);
+        on[i] = comp ? make_float2(so, o[8 + i]) : make_float2(o[i], so);
+      }
+      if (f < nfields) {
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-          const float se = __shfl_xor_sync(0xffffffffu, comp ? e[i] : e[8 + i], 1);
-          const float so = __shfl_xor_sync(0xffffffffu, comp ? o[i] : o[8 + i], 1);
-          en[i] = comp ? make_float2(se, e[8 + i]) : make_float2(e[i], se);
-          on[i] = comp ? make_float2(so, o[8 + i]) : make_float2(o[i], so);
-        }
-        if (f < nfields) {
-#pragma unroll
-          for (int i = 0; i < 8; i++) {
-            const int lat = lt * NL + c0 + comp * 8 + i;
-            if (lat < t.nh) {
-              dst[lat] = make_float2(en[i].x + on[i].x, en[i].y + on[i].y);
-              const int south = t.nlat - 1 - lat;
-              if (south != lat) dst[south] = make_float2(en[i].x - on[i].x, en[i].y - on[i].y);
-            }
+          const int lat = lt * NL + c0 + comp * 8 + i;
+          if (lat < t.nh) {
+            dst[lat] = make_float2(en[i].x + on[i].x, en[i].y + on[i].y);
+            const int south = t.nlat - 1 - lat;
+            if (south != lat) dst[south] = make_float2(en[i].x - on[i].x, en[i].y - on[i].y);
           }
         }
       }
     }
-    if (!ok && tid == 0) atomicExch(tc.err, 1);
-  }
+    return true;
+  };
+  ts_tc_persistent(smem, pp, S, stage, tmem, 2 * NL, sc, epilogue);
   ts_tc_fence_before();
   __syncthreads();
-  if (warp == 0) ts_tmem_free(tmem, ncols);
+  if (pp->bad && tid == 0) atomicExch(tc.err, 1);
+  if (warp == 0) ts_tmem_free(tmem, 512);
 }
 
 // ------------------------------------------------------------------ analysis
-//
-// grid = (ceil(nfields/per_cta), mmax+1, 2*ntile), block = 192; z = par*ntile
-// + ltile (empty tiles return at once).  per_cta <= 64 fields.  Stages: 2*16384
-// bytes of data operand + 2*N*128 bytes of table, over the latitude chunks.
-// Dynamic shared memory: max(S*stage, N*2*64*4) + 1024 + sizeof(TsTcPipe).
+struct TsAnalysSched {
+  const TsTcTab *tc;
+  int lmax, mmax, nfb, ntile;
+  const char *wimg;
+  TS_DEV int ntiles() const { return (mmax + 1) * 2 * ntile * nfb; }
+  TS_DEV void decode(int tile, int &m, int &par, int &lt, int &fb) const {
+    m = tile / (2 * ntile * nfb);
+    int r = tile - m * 2 * ntile * nfb;
+    fb = r % nfb;
+    r /= nfb;
+    par = r / ntile;
+    lt = r - par * ntile;
+  }
+  TS_DEV int cnt(int tile) const {
+    int m, par, lt, fb;
+    decode(tile, m, par, lt, fb);
+    return ts_atile_count(lmax, m, par, lt, tc->LTL);
+  }
+  TS_DEV int stages(int tile) const { return cnt(tile) > 0 ? tc->nLC : 0; }
+  TS_DEV int n(int tile) const { return max(16, ts_round16(cnt(tile))); }
+  TS_DEV unsigned table_bytes(int tile) const { return 2u * n(tile) * 128; }
+  TS_DEV const char *a_src(int tile, int c) const {
+    int m, par, lt, fb;
+    decode(tile, m, par, lt, fb);
+    return wimg + ((((long)m * nfb + fb) * 2 + par) * tc->nLC + c) * 16384;
+  }
+  TS_DEV const char *b_src(int tile, int c) const {
+    int m, par, lt, fb;
+    decode(tile, m, par, lt, fb);
+    return tc->anal + ts_atile_offset(*tc, lmax, m, par, lt) + (long)c * table_bytes(tile);
+  }
+  TS_DEV int d_col(int, int) const { return 0; }
+  TS_DEV bool first(int, int c) const { return c == 0; }
+};
+
+// grid = min(#SMs, tiles), block = 320, persistent.  Tiles with no l values
+// have no stages; their epilogue does nothing.  Dynamic shared memory:
+// S*(2*16384 + 2*Nmax*128) + Nmax*2*64*4 + 1024 + sizeof(TsTcPipe).  TMEM:
+// two buffers of 256 columns.
 template <class Epi>
 __global__ void __launch_bounds__(TS_TC_THREADS, 1)
-ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const float2 *__restrict__ g, long g_stride, Epi epi,
-                 int nfields, int per_cta, int S) {
+ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nfb, Epi epi,
+                 int nfields, int per_cta, int S, int nmax, int ntile) {
   extern __shared__ __align__(1024) char ts_smem_at[];
   char *smem = (char *)(((unsigned long long)ts_smem_at + 1023) & ~1023ull);
-  const int m = blockIdx.y;
-  const int ntile = gridDim.z / 2;
-  const int par = blockIdx.z / ntile, ltile = blockIdx.z - par * ntile;
-  const int cnt = ts_atile_count(t.lmax, m, par, ltile, tc.LTL);
-  if (cnt == 0) return;  // uniform for the CTA, before any barrier or allocation
-  const int N = ts_round16(cnt);
-  const int f0 = blockIdx.x * per_cta;
-  const int nf = min(per_cta, nfields - f0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long base = ts_lm_base(t.lmax, m);
-  const int bbytes = N * 128;
-  const int stage = 2 * 16384 + 2 * bbytes;
-  const int region = max(S * stage, N * 2 * TS_TC_FIELDS * 4);
-  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + region);
-  const unsigned ncols = ts_tmem_cols(N);
-  const long toff = ts_atile_offset(tc, t.lmax, m, par, ltile);
-  const int T = tc.nLC;
-
+  const unsigned stage = 2 * 16384 + 2 * nmax * 128;
+  float *sD = reinterpret_cast<float *>(smem + S * stage);
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + nmax * 2 * TS_TC_FIELDS * 4);
+  const TsAnalysSched sc{&tc, t.lmax, t.mmax, w_nfb, ntile, wimg};
   ts_tc_pipe_init(pp, S);
-  if (warp == 0) ts_tmem_alloc(&pp->tmem, ncols);
+  if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
   ts_tc_fence_before();
   __syncthreads();
   ts_tc_fence_after();
   const unsigned tmem = pp->tmem;
 
-  if (warp < 4) {
-    // ---- data operand: W = w (G_north +- G_south), lane = latitude of the chunk
-    const int k = lane, fg = warp;
-    for (int c = 0; c < T; c++) {
-      const int s = c % S, use = c / S;
-      const int lat = c * TS_TC_KCH + k;
-      const bool live = lat < t.nh;
-      const float w = live ? t.wq[lat] : 0.f;
-      const int south = t.nlat - 1 - lat;
-      float2 gn[16], gs[16];
+  // epilogue: TMEM -> shared [j][comp][field] -> Epi per (lm, comp)
+  unsigned ephase = 0;
+  auto epilogue = [&](int tile, unsigned tbase) -> bool {
+    const int cnt = sc.cnt(tile);
+    if (cnt == 0) return true;
+    int m, par, lt, fb;
+    sc.decode(tile, m, par, lt, fb);
+    const int N = ts_round16(cnt);
+    const int row = ts_epi_row(warp, lane), fl = row >> 1, comp = row & 1;
+    const unsigned lanebase = tbase + ((unsigned)((warp & 3) * 32) << 16);
+    if (!ts_epi_sync(pp, ephase)) return false;  // the previous tile's epi calls are done with sD
+    for (int c0 = 0; c0 < N; c0 += 16) {
+      float v[16];
+      ts_tmem_ld16(lanebase + (unsigned)c0, v);
 #pragma unroll
-      for (int i = 0; i < 16; i++) {
-        const int fl = fg * 16 + i;
-        gn[i] = gs[i] = make_float2(0.f, 0.f);
-        if (live && fl < nf) {
-          const float2 *src = g + (long)(f0 + fl) * g_stride + (long)m * t.nlat;
-          gn[i] = src[lat];
-          if (south != lat) gs[i] = src[south];
-        }
-      }
-      if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
-        ts_tc_flag(pp);
-        break;
-      }
-      char *ahi = smem + s * stage, *alo = ahi + 16384;
-#pragma unroll
-      for (int i = 0; i < 16; i++) {
-        const int fl = fg * 16 + i;
-        const float wr = par ? (gn[i].x - gs[i].x) * w : (gn[i].x + gs[i].x) * w;
-        const float wi = par ? (gn[i].y - gs[i].y) * w : (gn[i].y + gs[i].y) * w;
-        const float hr = ts_rna_tf32(wr), hi = ts_rna_tf32(wi);
-        *reinterpret_cast<float *>(ahi + ts_swz(2 * fl, k)) = hr;
-        *reinterpret_cast<float *>(alo + ts_swz(2 * fl, k)) = ts_rna_tf32(wr - hr);
-        *reinterpret_cast<float *>(ahi + ts_swz(2 * fl + 1, k)) = hi;
-        *reinterpret_cast<float *>(alo + ts_swz(2 * fl + 1, k)) = ts_rna_tf32(wi - hi);
-      }
-      ts_fence_proxy_async();
-      __syncwarp();
-      if (lane == 0) ts_mbar_arrive(&pp->full[s]);
+      for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_FIELDS + fl] = v[i];
     }
-  } else if (warp == 4) {
-    if (lane == 0) {
-      for (int c = 0; c < T; c++) {
-        const int s = c % S, use = c / S;
-        if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
-          ts_tc_flag(pp);
-          break;
-        }
-        ts_mbar_arrive_tx(&pp->full[s], 2 * bbytes);
-        ts_bulk_g2s(smem + s * stage + 2 * 16384, tc.anal + toff + (long)c * 2 * bbytes,
-                    2 * bbytes, &pp->full[s]);
-      }
-    }
-  } else {
-    if (lane == 0) {
-      const unsigned idesc = ts_idesc_tf32(N);
-      for (int c = 0; c < T; c++) {
-        const int s = c % S, use = c / S;
-        if (!ts_mbar_wait(&pp->full[s], use & 1, TS_TC_WAIT_LIMIT)) {
-          ts_tc_flag(pp);
-          break;
-        }
-        ts_tc_fence_after();
-        const unsigned ahi = ts_smem_u32(smem + s * stage), alo = ahi + 16384;
-        const unsigned bhi = ahi + 2 * 16384, blo = bhi + bbytes;
-#pragma unroll
-        for (int kk = 0; kk < 4; kk++) {
-          const unsigned acc = (c > 0 || kk > 0) ? 1u : 0u;
-          ts_mma_tf32(tmem, ts_umma_desc(ahi + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, acc);
-          ts_mma_tf32(tmem, ts_umma_desc(ahi + kk * 32), ts_umma_desc(blo + kk * 32), idesc, 1u);
-          ts_mma_tf32(tmem, ts_umma_desc(alo + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, 1u);
-        }
-        ts_mma_commit(&pp->empty[s]);
-      }
-      ts_mma_commit(&pp->done);
-    }
-  }
-
-  // ---- epilogue: TMEM -> shared [j][comp][field] -> Epi per (lm, comp)
-  bool ok = true;
-  if (warp < 4) {
-    ok = ts_mbar_wait(&pp->done, 0, TS_TC_WAIT_LIMIT) && !pp->bad;
-    ts_tc_fence_after();
-    if (ok) {
-      float *sD = reinterpret_cast<float *>(smem);
-      const int row = warp * 32 + lane, fl = row >> 1, comp = row & 1;
-      for (int c0 = 0; c0 < N; c0 += 16) {
-        float v[16];
-        ts_tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
-#pragma unroll
-        for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_FIELDS + fl] = v[i];
-      }
-    }
-  }
-  ts_tc_fence_before();
-  ok = __syncthreads_and(ok || warp >= 4) && !pp->bad;
-  if (ok) {
-    const float *sD = reinterpret_cast<const float *>(smem);
-    for (int idx = tid; idx < cnt * 2; idx += blockDim.x) {
+    if (!ts_epi_sync(pp, ephase)) return false;
+    const int f0 = fb * per_cta;
+    const int nf = min(per_cta, nfields - f0);
+    const long base = ts_lm_base(t.lmax, m);
+    for (int idx = (warp & 3) * 32 + lane; idx < cnt * 2; idx += 128) {
       const int j = idx >> 1, cp = idx & 1;
-      const int l = m + par + 2 * (ltile * tc.LTL + j);
+      const int l = m + par + 2 * (lt * tc.LTL + j);
       epi(base + (l - m), cp, sD + (j * 2 + cp) * TS_TC_FIELDS, f0, nf, TS_TC_FIELDS);
     }
-  } else if (tid == 0) {
-    atomicExch(tc.err, 1);
-  }
+    return true;
+  };
+  ts_tc_persistent(smem, pp, S, stage, tmem, 256, sc, epilogue);
   ts_tc_fence_before();
   __syncthreads();
-  if (warp == 0) ts_tmem_free(tmem, ncols);
+  if (pp->bad && tid == 0) atomicExch(tc.err, 1);
+  if (warp == 0) ts_tmem_free(tmem, 512);
 }

@@ -74,6 +74,12 @@ struct TsLegTab {
   int lmax, mmax, nlat, nh;  // nh = ceil(nlat/2): latitudes a recurrence walks
 };
 
+// byte offset of element (row r, k) in a K-major 128B-swizzled tile of
+// 32-float rows: 8-row groups of 1024 bytes, 16-byte chunk index XOR row % 8
+TS_DEV int ts_swz_img(int r, int k) {
+  return (r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 2) ^ (r & 7))) << 4) + ((k & 3) << 2);
+}
+
 // A set of coefficient fields read by the Legendre synthesis: field f is
 // species s = f % nper of instance i = f / nper, at base[s] + i*inst_stride[s].
 #define TS_MAXIO 8
@@ -105,6 +111,23 @@ struct TsTcTab {
   int LTL;                  // analysis l-tile (per parity), <= 256
   int nLC;                  // analysis latitude chunks of 32
   int *err;                 // set to 1 when a bounded wait gives up
+  const int *chunk_prefix;  // synthesis k-chunks (both parities) before m, mmax+2 entries
+  const int *chunk_m;       // chunk -> m
+  const int *chunk_pc;      // chunk -> (parity << 16) | chunk-of-parity
+  int nchunks;
+};
+
+// The data operands of the tensor-core Legendre stage, kept in HBM as raw fp32
+// in the shared-memory byte image the MMA reads (16 KB blocks: 128 rows =
+// 64 fields x re|im, 32 k, K-major 128-byte swizzle):
+//   q: synthesis, block (chunk_prefix[m] + chunk, field block), k -> l
+//   w: analysis, block ((m*w_nfb + field block)*2 + parity)*nLC + latitude
+//      chunk, k -> northern latitude, value w*(G_north +- G_south)
+struct TsTcImg {
+  char *q;
+  int q_nfb;
+  char *w;
+  int w_nfb, w_fpb;  // field blocks and fields per block (<= 64) of w
 };
 
 // Grid-phase I/O of a compiled model (see ts_fourier_phase in fourier.cuh).
@@ -118,6 +141,10 @@ struct TsPhaseIO {
   long gout_stride[TS_MAXIO];
   const float *prm;
   int nprm;
+  // tensor-core plans: the analysis outputs go to the W image instead of gm
+  char *wimg;
+  int w_nfb, w_fpb, w_nlc, nh;
+  const float *wq;
 };
 
 // Spectral-side I/O of a compiled model's generated code: inputs and outputs

@@ -57,6 +57,7 @@ struct Stage {
   std::vector<Ref> in, out;
   int nsyn = 0, nana = 0;
   int lb = 0, F = 1, K = 1, W = 1, per_cta = 1, r1 = 0;
+  bool wimg = false;  // tensor-core plan: the phase writes the W image itself
   size_t smem = 0;
   std::string label;  // one line, for describe()
   std::string src;    // generated CUDA of this stage
@@ -163,7 +164,7 @@ struct ts_model_s {
   Program prog[2];  // init, step
   float *d_prm = nullptr;
   std::vector<float> h_prm;
-  ts_dbuf fm, gm, stash;
+  ts_dbuf fm, gm, stash, qimg, wimg;
   cudaLibrary_t lib = nullptr;
   int last_ran = 0, stashed_ran = 0;
   std::string source;
@@ -412,9 +413,13 @@ void schedule(ts_model m, Program &P, bool is_step) {
         src << "    out[" << A.size() + o << "] = " << em.name.at(gout[o]) << ";\n";
       src << "  }\n};\n";
       const int r1 = ts_fft_r1(p);
-      st.expr = r1 ? "ts_fourier_phase_r<" + pn + ", " + std::to_string(r1) + ">"
-                   : "ts_fourier_phase<" + pn + ">";
+      const bool tcw = p->precision != TS_PREC_FP32 && r1 && !A.empty();
+      st.expr = tcw  ? "ts_fourier_phase_rw<" + pn + ", " + std::to_string(r1) + ">"
+                : r1 ? "ts_fourier_phase_r<" + pn + ", " + std::to_string(r1) + ">"
+                     : "ts_fourier_phase<" + pn + ">";
       st.r1 = r1;
+      st.wimg = tcw;
+      if (tcw) st.per_cta = (int)A.size() * (TS_TC_FIELDS / (int)A.size());
       st.label = "phase   " + std::to_string(S.size()) + " synth, " + std::to_string(G.size()) +
                  " grid statement(s), " + std::to_string(A.size()) + " analys";
       st.src = src.str();
@@ -462,6 +467,7 @@ void schedule(ts_model m, Program &P, bool is_step) {
     Stage st;
     st.kind = Stage::LegAnalys;
     st.nana = (int)A.size();
+    st.wimg = P.stages.back().kind == Stage::Phase && P.stages.back().wimg;
     for (int v : sin) st.in.push_back(ref[v]);
     for (int v : sout) st.out.push_back(ref[v]);
     const bool tc = p->precision != TS_PREC_FP32;
@@ -640,7 +646,10 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
           q.inst_stride[i] = stride / 2;
         }
         q.nper = s.nsyn;
-        ts_launch_leg_synth_fields(p, q, fm, field, B * s.nsyn, st);
+        if (p->precision != TS_PREC_FP32)
+          ts_launch_leg_synth_tc(p, q, fm, field, B * s.nsyn, st, &m->qimg);
+        else
+          ts_launch_leg_synth_fields(p, q, fm, field, B * s.nsyn, st);
         break;
       }
       case Stage::Phase: {
@@ -654,9 +663,17 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
           io.gout[i] = resolve(m, P, s.out[i], &io.gout_stride[i]);
         io.prm = m->d_prm;
         io.nprm = (int)m->params.size();
+        io.nh = p->nh;
+        if (s.wimg) {
+          io.wimg = (char *)m->wimg.p;
+          io.w_fpb = s.per_cta;
+          io.w_nfb = (B * s.nana + s.per_cta - 1) / s.per_cta;
+          io.w_nlc = (p->nh + 31) / 32;
+          io.wq = p->d_wq;
+        }
         TsFftTab ft = p->fft;
         void *args[] = {&ft, &io};
-        dim3 grid((p->nlat + s.lb - 1) / s.lb, B);
+        dim3 grid(s.wimg ? (p->nh + s.lb - 1) / s.lb : (p->nlat + s.lb - 1) / s.lb, B);
         TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(32 * s.lb), args, s.smem, st));
         break;
       }
@@ -672,9 +689,15 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
         if (p->precision != TS_PREC_FP32) {
           TsTcTab tc = ts_tc_tab(p);
           int S = ts_tc_analys_stages(p);
-          void *args[] = {&leg, &tc, &g, &gs, &epi, &nfields, &per_cta, &S};
-          dim3 grid((nfields + per_cta - 1) / per_cta, p->mmax + 1, 2 * ts_tc_ntile(p));
-          TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(192), args, s.smem, st));
+          int nmax = ts_tc_analys_nmax(p);
+          int ntile = ts_tc_ntile(p);
+          int w_nfb = (nfields + per_cta - 1) / per_cta;
+          if (!s.wimg)  // the phase wrote G: fold it into the W image first
+            ts_launch_wimage(p, gm, field, nfields, per_cta, (char *)m->wimg.p, st);
+          const char *wimg = (const char *)m->wimg.p;
+          void *args[] = {&leg, &tc, &wimg, &w_nfb, &epi, &nfields, &per_cta, &S, &nmax, &ntile};
+          const int ctas = ts_tc_ctas(p, (long)(p->mmax + 1) * 2 * ntile * w_nfb);
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern, dim3(ctas), dim3(320), args, s.smem, st));
         } else {
           void *args[] = {&leg, &g, &gs, &epi, &nfields, &per_cta};
           dim3 grid(p->mmax + 1, (nfields + per_cta - 1) / per_cta);
@@ -704,7 +727,9 @@ void finish_shapes(ts_model m) {
     for (auto &s : P.stages) {
       if (s.kind == Stage::Phase) {
         const int nrows = s.nsyn + s.nana + 1;
-        s.lb = s.r1 ? ts_rfft_lb(p, m->batch, 1, &s.smem) : ts_fourier_lb(p, m->batch, nrows, &s.smem);
+        s.lb = s.wimg ? ts_rfft_np(p, m->batch, s.nana, &s.smem)
+               : s.r1 ? ts_rfft_lb(p, m->batch, 1, &s.smem)
+                      : ts_fourier_lb(p, m->batch, nrows, &s.smem);
       } else if (s.kind == Stage::LegAnalys) {
         s.smem = p->precision != TS_PREC_FP32 ? ts_tc_analys_smem(p) : ts_analys_smem(p, s.F, s.W);
       }
@@ -723,6 +748,8 @@ void free_model(ts_model m) {
   m->fm.release();
   m->gm.release();
   m->stash.release();
+  m->qimg.release();
+  m->wimg.release();
   if (m->lib) cudaLibraryUnload(m->lib);
 }
 
@@ -872,6 +899,17 @@ int ts_model_compile(ts_plan plan, const char *source, const char *const *state,
     const int nana = std::max({m->prog[0].nana_max, m->prog[1].nana_max, 1});
     m->fm.ensure(sizeof(float2) * field * nsyn * batch);
     m->gm.ensure(sizeof(float2) * field * nana * batch);
+    if (plan->precision != TS_PREC_FP32) {
+      size_t wb = 0;
+      for (auto &P : m->prog)
+        for (auto &st : P.stages)
+          if (st.kind == Stage::LegAnalys)
+            wb = std::max(wb, ts_tc_wimg_bytes(plan, batch * st.nana, st.per_cta));
+      m->wimg.ensure(std::max<size_t>(wb, 16));
+      TS_CUDA(cudaMemset(m->wimg.p, 0, m->wimg.cap));
+      m->qimg.ensure(ts_tc_qimg_bytes(plan, batch * nsyn));
+      TS_CUDA(cudaMemset(m->qimg.p, 0, m->qimg.cap));
+    }
     m->stash.ensure(sizeof(float) * 2 * nlm * batch * nstate);
     m->h_prm.assign((size_t)std::max(nparams, 1) * batch, 0.0f);
     m->d_prm = dalloc((long)m->h_prm.size());

@@ -70,7 +70,14 @@ extern "C" int ts_sht_synth_noalloc(ts_plan p, const float *qlm, float *spat, in
     // The Legendre stage writes every (field, m, latitude) entry the Fourier
     // stage then reads, so nothing left in the array by an earlier call is used.
     cudaStream_t s = ts_pick_stream(ctx, stream);
-    ts_launch_leg_synth(p, (const float2 *)qlm, p->nlm, fm, fm_stride, batch, s);
+    // The FP32 Legendre kernels read the coefficients as they are; the
+    // tensor-core path would first relayout them into a plan-owned operand
+    // image grown on demand, so this entry point always takes the FP32 path.
+    TsFields qf{};
+    qf.base[0] = (const float2 *)qlm;
+    qf.inst_stride[0] = p->nlm;
+    qf.nper = 1;
+    ts_launch_leg_synth_plain(p, qf, fm, fm_stride, batch, s);
     ts_launch_fourier_synth(p, fm, fm_stride, spat, (long)p->nlat * p->nphi, batch, s);
     return TS_OK;
   } catch (const ts_exc &e) {

@@ -93,6 +93,9 @@ void ts_launch_fourier_analys(ts_plan p, const float *spat, long spat_stride, fl
                               long g_stride, int nfields, cudaStream_t s);
 void ts_launch_leg_synth_fields(ts_plan p, const TsFields &q, float2 *fm, long fm_stride,
                                 int nfields, cudaStream_t s);
+// the FP32 on-the-fly recurrence whatever the plan's precision (allocates nothing)
+void ts_launch_leg_synth_plain(ts_plan p, const TsFields &q, float2 *fm, long fm_stride,
+                               int nfields, cudaStream_t s);
 // analysis launch shape: fields per CTA F (template), latitudes per thread K,
 // warps W; groups = fields handled per CTA (a multiple of `per_inst`)
 void ts_analys_shape(ts_plan p, int nfields, int per_inst, int *F, int *K, int *W, int *per_cta);
@@ -114,9 +117,29 @@ size_t ts_tc_synth_smem(ts_plan p);
 size_t ts_tc_analys_smem(ts_plan p);
 int ts_tc_synth_stages(ts_plan p);
 int ts_tc_analys_stages(ts_plan p);
+int ts_tc_analys_nmax(ts_plan p);
+struct TsTcGeom {
+  int NL, nLT, LTL, ntile;
+};
+TsTcGeom ts_tc_geom(ts_plan p);
+int ts_tc_ctas(ts_plan p, long ntiles);
+// TC synthesis: fields -> q image (qbuf, or the plan's) -> fm
 void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fm_stride, int nfields,
-                            cudaStream_t s);
+                            cudaStream_t s, ts_dbuf *qbuf = nullptr);
+// TC analysis from G in the gm layout (stage-level)
 void ts_launch_leg_analys_tc(ts_plan p, const float2 *g, long g_stride, float2 *q, long q_stride,
                              int nfields, cudaStream_t s);
+// TC analysis from the grid: spat -> w image -> q
+void ts_analys_tc_full(ts_plan p, const float *spat, long spat_stride, float *qlm, int nfields,
+                       cudaStream_t s);
+size_t ts_tc_qimg_bytes(ts_plan p, int nfields);
+size_t ts_tc_wimg_bytes(ts_plan p, int nfields, int fpb);
+void ts_launch_wimage(ts_plan p, const float2 *g, long gs, int nf, int fpb, char *img,
+                      cudaStream_t s);
+// spat -> w image with the paired register FFT; false when the grid does not allow it
+bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb,
+                                char *wimg, cudaStream_t s);
+// north/south pairs per CTA of the paired Fourier kernels, and their shared memory
+int ts_rfft_np(ts_plan p, int nblocks_y, int ntiles_out, size_t *smem);
 int ts_tc_check_error(ts_plan p);
 void ts_kernel_attrs_once(ts_ctx ctx);

@@ -298,6 +298,11 @@ void ts_kernel_attrs_once(ts_ctx ctx) {
 void ts_launch_leg_synth_fields(ts_plan p, const TsFields &q, float2 *fm, long fs, int nf,
                                 cudaStream_t s) {
   if (p->precision != TS_PREC_FP32) return ts_launch_leg_synth_tc(p, q, fm, fs, nf, s);
+  ts_launch_leg_synth_plain(p, q, fm, fs, nf, s);
+}
+
+void ts_launch_leg_synth_plain(ts_plan p, const TsFields &q, float2 *fm, long fs, int nf,
+                               cudaStream_t s) {
   const int bd = p->nh >= 128 ? 64 : 32;
   auto go = [&](auto Fc) {
     constexpr int F = decltype(Fc)::value;
@@ -389,7 +394,40 @@ int ts_rfft_lb(ts_plan p, int nblocks_y, int nrowbuf, size_t *smem) {
   return lb;
 }
 
+// pairs per paired CTA: tiles tw | twr | tin (or tN) | ntiles_out*2 x [NP][P] | rowbuf
+int ts_rfft_np(ts_plan p, int nblocks_y, int ntiles_out, size_t *smem) {
+  const int nh = p->nh, P = p->mmax + 2, H = p->fft.H;
+  int np = 8;
+  auto bytes = [&](int n) {
+    return sizeof(float2) * ((size_t)p->nphi + H + (size_t)n * P * (1 + 2 * ntiles_out) +
+                             (size_t)n * H);
+  };
+  for (; np > 1; np >>= 1) {
+    const long ctas = (long)nblocks_y * ((nh + np - 1) / np);
+    if (bytes(np) <= p->ctx->smem_optin / 2 && ctas >= 2L * p->ctx->sm_count) break;
+  }
+  *smem = bytes(np);
+  TS_REQUIRE(*smem <= p->ctx->smem_optin, TS_ERR_UNSUPPORTED, "grid too large for the paired FFT");
+  return np;
+}
+
 namespace {
+template <int R1>
+void ranalys_w(ts_plan p, const float *spat, long ss, int nf, int fpb, char *wimg, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    TS_CUDA(cudaFuncSetAttribute(ts_fourier_analys_rw<R1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)p->ctx->smem_optin));
+    attr = true;
+  }
+  size_t smem;
+  const int np = ts_rfft_np(p, nf, 1, &smem);
+  const int nlc = (p->nh + 31) / 32;
+  dim3 grid((p->nh + np - 1) / np, nf);
+  ts_fourier_analys_rw<R1><<<grid, 32 * np, smem, s>>>(p->fft, spat, ss, p->d_wq, wimg,
+                                                       (nf + fpb - 1) / fpb, fpb, nlc, p->nh);
+  TS_CUDA(cudaGetLastError());
+}
 template <int R1>
 void rsynth(ts_plan p, const float2 *fm, long fs, float *spat, long ss, int nf, cudaStream_t s) {
   static bool attr = false;
@@ -431,6 +469,22 @@ void ranalys(ts_plan p, const float *spat, long ss, float2 *g, long gs, int nf, 
     case 24: return F<24>(__VA_ARGS__);   \
   }
 }  // namespace
+
+bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb,
+                                char *wimg, cudaStream_t s) {
+  switch (ts_fft_r1(p)) {
+    case 1: ranalys_w<1>(p, spat, ss, nf, fpb, wimg, s); return true;
+    case 2: ranalys_w<2>(p, spat, ss, nf, fpb, wimg, s); return true;
+    case 3: ranalys_w<3>(p, spat, ss, nf, fpb, wimg, s); return true;
+    case 4: ranalys_w<4>(p, spat, ss, nf, fpb, wimg, s); return true;
+    case 6: ranalys_w<6>(p, spat, ss, nf, fpb, wimg, s); return true;
+    case 8: ranalys_w<8>(p, spat, ss, nf, fpb, wimg, s); return true;
+    case 12: ranalys_w<12>(p, spat, ss, nf, fpb, wimg, s); return true;
+    case 16: ranalys_w<16>(p, spat, ss, nf, fpb, wimg, s); return true;
+    case 24: ranalys_w<24>(p, spat, ss, nf, fpb, wimg, s); return true;
+    default: return false;
+  }
+}
 
 void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, long ss, int nf,
                              cudaStream_t s) {

@@ -1,5 +1,6 @@
 // Tensor-core Legendre tables (FP64 on the GPU) and launchers.
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "kernels/leg_f32.cuh"
@@ -92,10 +93,29 @@ int kpar_h(int lmax, int m, int par) { return (lmax - m + 1 + 1 - par) / 2; }
 
 }  // namespace
 
+// Tile geometry of the tensor-core kernels, from the plan's sizes alone (so
+// the model compiler can size shared memory without the tables).  TS_TC_NL
+// (the synthesis latitude tile, a multiple of 16 <= 128) and TS_TC_LTL (the
+// analysis degree tile, a multiple of 16 <= 256) tune it, like the
+// reference's SHT_* knobs (src/sht/sht.ts:47-56).
+TsTcGeom ts_tc_geom(ts_plan p) {
+  TsTcGeom g;
+  int nl_cap = 96;  // two accumulator buffers of 2*NL columns fit in 512
+  if (const char *e = getenv("TS_TC_NL")) nl_cap = std::max(16, std::min(128, atoi(e) & ~15));
+  g.NL = std::min(nl_cap, ((p->nh + 15) / 16) * 16);
+  g.nLT = (p->nh + g.NL - 1) / g.NL;
+  g.LTL = 128;
+  if (const char *e = getenv("TS_TC_LTL")) g.LTL = std::max(16, std::min(256, atoi(e) & ~15));
+  g.ntile = (kpar_h(p->lmax, 0, 0) + g.LTL - 1) / g.LTL;
+  return g;
+}
+
 struct ts_tc_tables {
   char *synth = nullptr, *anal = nullptr;
   long *synth_off = nullptr, *anal_off = nullptr;
   int *err = nullptr;
+  int *chunk_prefix = nullptr, *chunk_m = nullptr, *chunk_pc = nullptr;
+  ts_dbuf qimg, wimg, gscratch;  // operand images and a G scratch of the standalone transforms
   TsTcTab tab{};
   size_t bytes = 0;
   int ntile = 1;  // analysis l tiles per parity (grid.z = 2*ntile)
@@ -105,20 +125,25 @@ void ts_tc_init(ts_plan p) {
   auto *t = new ts_tc_tables();
   p->tc = t;
   const int nh = p->nh;
-  int NL = ((nh + 15) / 16) * 16;
-  if (NL > 192) NL = 192;
-  const int nLT = (nh + NL - 1) / NL;
-  const int LTL = 256;
+  const TsTcGeom gm = ts_tc_geom(p);
+  const int NL = gm.NL, nLT = gm.nLT, LTL = gm.LTL;
   const int nLC = (nh + TS_TC_KCH - 1) / TS_TC_KCH;
   std::vector<long> soff(p->mmax + 2), aoff(p->mmax + 2);
+  std::vector<int> cpre(p->mmax + 2), cm, cpc;
   long s = 0, a = 0;
   for (int m = 0; m <= p->mmax; m++) {
     soff[m] = s;
     aoff[m] = a;
+    cpre[m] = (int)cm.size();
     int nch = 0;
     for (int par = 0; par < 2; par++) {
       const int kp = kpar_h(p->lmax, m, par);
-      nch += (kp + TS_TC_KCH - 1) / TS_TC_KCH;
+      const int nc = (kp + TS_TC_KCH - 1) / TS_TC_KCH;
+      for (int c = 0; c < nc; c++) {
+        cm.push_back(m);
+        cpc.push_back((par << 16) | c);
+      }
+      nch += nc;
       for (int lt0 = 0; lt0 < kp; lt0 += LTL) {
         const int cnt = std::min(kp, lt0 + LTL) - lt0;
         a += (long)nLC * 2 * (((cnt + 15) / 16) * 16) * 128;
@@ -128,6 +153,13 @@ void ts_tc_init(ts_plan p) {
   }
   soff[p->mmax + 1] = s;
   aoff[p->mmax + 1] = a;
+  cpre[p->mmax + 1] = (int)cm.size();
+  TS_CUDA(cudaMalloc(&t->chunk_prefix, sizeof(int) * cpre.size()));
+  TS_CUDA(cudaMalloc(&t->chunk_m, sizeof(int) * cm.size()));
+  TS_CUDA(cudaMalloc(&t->chunk_pc, sizeof(int) * cpc.size()));
+  TS_CUDA(cudaMemcpy(t->chunk_prefix, cpre.data(), sizeof(int) * cpre.size(), cudaMemcpyHostToDevice));
+  TS_CUDA(cudaMemcpy(t->chunk_m, cm.data(), sizeof(int) * cm.size(), cudaMemcpyHostToDevice));
+  TS_CUDA(cudaMemcpy(t->chunk_pc, cpc.data(), sizeof(int) * cpc.size(), cudaMemcpyHostToDevice));
   t->ntile = (kpar_h(p->lmax, 0, 0) + LTL - 1) / LTL;
   TS_CUDA(cudaMalloc(&t->synth, s));
   TS_CUDA(cudaMalloc(&t->anal, a));
@@ -150,6 +182,10 @@ void ts_tc_init(ts_plan p) {
   tc.LTL = LTL;
   tc.nLC = nLC;
   tc.err = t->err;
+  tc.chunk_prefix = t->chunk_prefix;
+  tc.chunk_m = t->chunk_m;
+  tc.chunk_pc = t->chunk_pc;
+  tc.nchunks = (int)cm.size();
   dim3 grid((nh + 63) / 64, p->mmax + 1);
   ts_k_tc_tables<<<grid, 64, 0, p->ctx->stream>>>(p->lmax, p->mmax, nh, p->d_x64, p->d_ab64,
                                                   p->d_amm64, tc, t->synth, t->anal);
@@ -161,8 +197,11 @@ void ts_tc_free(ts_plan p) {
   auto *t = static_cast<ts_tc_tables *>(p->tc);
   if (!t) return;
   for (void *q : {(void *)t->synth, (void *)t->anal, (void *)t->synth_off, (void *)t->anal_off,
-                  (void *)t->err})
+                  (void *)t->err, (void *)t->chunk_prefix, (void *)t->chunk_m, (void *)t->chunk_pc})
     if (q) cudaFree(q);
+  t->qimg.release();
+  t->wimg.release();
+  t->gscratch.release();
   delete t;
   p->tc = nullptr;
 }
@@ -171,36 +210,123 @@ const TsTcTab &ts_tc_tab(ts_plan p) { return static_cast<ts_tc_tables *>(p->tc)-
 int ts_tc_ntile(ts_plan p) { return static_cast<ts_tc_tables *>(p->tc)->ntile; }
 size_t ts_tc_bytes(ts_plan p) { return p->tc ? static_cast<ts_tc_tables *>(p->tc)->bytes : 0; }
 
-// pipeline depth and shared memory of the two kernels
+// pipeline depth and shared memory of the two persistent kernels
 namespace {
 const size_t kSmemBudget = 227 * 1024 - 2048;
+size_t synth_stage(ts_plan p) { return 2 * 16384 + 2 * (size_t)ts_tc_geom(p).NL * 128; }
 int synth_stages(ts_plan p) {
-  const size_t stage = 2 * 16384 + 2 * (size_t)ts_tc_tab(p).NL * 128;
-  return (int)std::min<size_t>(TS_TC_MAXSTAGE, kSmemBudget / stage);
+  return (int)std::min<size_t>(TS_TC_MAXSTAGE, kSmemBudget / synth_stage(p));
 }
-int analys_N(ts_plan p) { return std::min(256, ((kpar_h(p->lmax, 0, 0) + 15) / 16) * 16); }
+int analys_N(ts_plan p) { return std::min(ts_tc_geom(p).LTL, ((kpar_h(p->lmax, 0, 0) + 15) / 16) * 16); }
+size_t analys_stage(ts_plan p) { return 2 * 16384 + 2 * (size_t)analys_N(p) * 128; }
+size_t analys_staging(ts_plan p) { return (size_t)analys_N(p) * 2 * TS_TC_FIELDS * 4; }
 }  // namespace
 
 int ts_tc_synth_stages(ts_plan p) { return synth_stages(p); }
 int ts_tc_analys_stages(ts_plan p) {
-  // the planner's dry run has no tables: derive from the grid alone
-  const size_t stage = 2 * 16384 + 2 * (size_t)analys_N(p) * 128;
-  return (int)std::min<size_t>(TS_TC_MAXSTAGE, kSmemBudget / stage);
+  return (int)std::min<size_t>(TS_TC_MAXSTAGE, (kSmemBudget - analys_staging(p)) / analys_stage(p));
 }
+int ts_tc_analys_nmax(ts_plan p) { return analys_N(p); }
 
 size_t ts_tc_synth_smem(ts_plan p) {
-  const size_t stage = 2 * 16384 + 2 * (size_t)ts_tc_tab(p).NL * 128;
-  return synth_stages(p) * stage + 1024 + sizeof(TsTcPipe);
+  return synth_stages(p) * synth_stage(p) + 1024 + sizeof(TsTcPipe);
 }
 
 size_t ts_tc_analys_smem(ts_plan p) {
-  const int N = analys_N(p);
-  const size_t stage = 2 * 16384 + 2 * (size_t)N * 128;
-  return std::max(ts_tc_analys_stages(p) * stage, (size_t)N * 2 * TS_TC_FIELDS * 4) + 1024 +
-         sizeof(TsTcPipe);
+  return ts_tc_analys_stages(p) * analys_stage(p) + analys_staging(p) + 1024 + sizeof(TsTcPipe);
 }
 
-void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fs, int nf,
+int ts_tc_ctas(ts_plan p, long ntiles) {
+  return (int)std::max<long>(1, std::min<long>(p->ctx->sm_count, ntiles));
+}
+
+// ---------------------------------------------------------- operand images
+
+namespace {
+
+// Q (fields) -> raw fp32 synthesis image; grid = (nchunks, q_nfb), block =
+// 256: warp -> 8 fields, lane -> k (coalesced 128-byte image rows)
+__global__ void ts_k_qimage(TsLegTab t, TsTcTab tc, TsFields q, int nfields, char *img,
+                            int nfb) {
+  const int c = blockIdx.x, fb = blockIdx.y;
+  const int m = tc.chunk_m[c], pc = tc.chunk_pc[c];
+  const int par = pc >> 16, cc = pc & 0xffff;
+  const int kp = ts_kpar(t.lmax, m, par);
+  const long base = ts_lm_base(t.lmax, m);
+  char *blk = img + ((long)c * nfb + fb) * 16384;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = cc * TS_TC_KCH + lane;
+  for (int fl = warp; fl < TS_TC_FIELDS; fl += 8) {
+    const int f = fb * TS_TC_FIELDS + fl;
+    float2 v = make_float2(0.f, 0.f);
+    if (f < nfields && j < kp) v = ts_field(q, f)[base + par + 2 * j];
+    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl, lane)) = v.x;
+    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl + 1, lane)) = v.y;
+  }
+}
+
+// G[field][m][lat] -> raw fp32 W image (the fold the Fourier analysis does
+// itself when it can: see ts_fourier_analys_rw).  grid = (nLC, nfb*2, mmax+1),
+// block = 256: warp -> 8 fields, lane -> latitude of the chunk
+__global__ void ts_k_wimage(TsLegTab t, const float2 *g, long gs, int nfields, int fpb, int nfb,
+                            int nlc, char *img) {
+  const int c = blockIdx.x, fb = blockIdx.y >> 1, par = blockIdx.y & 1, m = blockIdx.z;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lat = c * TS_TC_KCH + lane;
+  const bool live = lat < t.nh;
+  const float w = live ? t.wq[lat] : 0.f;
+  const int south = t.nlat - 1 - lat;
+  char *blk = img + ((((long)m * nfb + fb) * 2 + par) * nlc + c) * 16384;
+  for (int fl = warp; fl < TS_TC_FIELDS; fl += 8) {
+    const int f = fb * fpb + fl;
+    float2 gn = make_float2(0.f, 0.f), gsv = make_float2(0.f, 0.f);
+    if (live && fl < fpb && f < nfields) {
+      const float2 *src = g + (long)f * gs + (long)m * t.nlat;
+      gn = src[lat];
+      if (south != lat) gsv = src[south];
+    }
+    const float a = par ? gn.x - gsv.x : gn.x + gsv.x;
+    const float b = par ? gn.y - gsv.y : gn.y + gsv.y;
+    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl, lane)) = a * w;
+    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl + 1, lane)) = b * w;
+  }
+}
+
+void ensure_zeroed(ts_dbuf &b, size_t bytes) {
+  if (bytes <= b.cap) return;
+  b.ensure(bytes);
+  TS_CUDA(cudaMemset(b.p, 0, b.cap));
+}
+
+}  // namespace
+
+size_t ts_tc_qimg_bytes(ts_plan p, int nfields) {
+  const long nfb = (nfields + TS_TC_FIELDS - 1) / TS_TC_FIELDS;
+  return (size_t)ts_tc_tab(p).nchunks * nfb * 16384;
+}
+
+size_t ts_tc_wimg_bytes(ts_plan p, int nfields, int fpb) {
+  const long nfb = (nfields + fpb - 1) / fpb;
+  return (size_t)(p->mmax + 1) * nfb * 2 * ts_tc_tab(p).nLC * 16384;
+}
+
+void ts_launch_qimage(ts_plan p, const TsFields &q, int nf, char *img, cudaStream_t s) {
+  const int nfb = (nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS;
+  dim3 grid(ts_tc_tab(p).nchunks, nfb);
+  ts_k_qimage<<<grid, 256, 0, s>>>(p->leg, ts_tc_tab(p), q, nf, img, nfb);
+  TS_CUDA(cudaGetLastError());
+}
+
+void ts_launch_wimage(ts_plan p, const float2 *g, long gs, int nf, int fpb, char *img,
+                      cudaStream_t s) {
+  const int nfb = (nf + fpb - 1) / fpb;
+  const int nlc = ts_tc_tab(p).nLC;
+  dim3 grid(nlc, nfb * 2, p->mmax + 1);
+  ts_k_wimage<<<grid, 256, 0, s>>>(p->leg, g, gs, nf, fpb, nfb, nlc, img);
+  TS_CUDA(cudaGetLastError());
+}
+
+void ts_launch_synth_tc_img(ts_plan p, const char *qimg, int nf, float2 *fm, long fs,
                             cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
@@ -209,13 +335,24 @@ void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fs, i
     attr = true;
   }
   const TsTcTab &tc = ts_tc_tab(p);
-  dim3 grid((nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS, p->mmax + 1, tc.nLT);
-  ts_leg_synth_tc<<<grid, TS_TC_THREADS, ts_tc_synth_smem(p), s>>>(p->leg, tc, q, fm, fs, nf,
-                                                                    synth_stages(p));
+  const int nfb = (nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS;
+  const int ctas = ts_tc_ctas(p, (long)(p->mmax + 1) * tc.nLT * nfb);
+  ts_leg_synth_tc<<<ctas, TS_TC_THREADS, ts_tc_synth_smem(p), s>>>(p->leg, tc, qimg, nfb, fm, fs,
+                                                                   nf, synth_stages(p));
   TS_CUDA(cudaGetLastError());
 }
 
-void ts_launch_leg_analys_tc(ts_plan p, const float2 *g, long gs, float2 *out, long os, int nf,
+// fields -> q image (caller's buffer, or the plan's) -> fm
+void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fs, int nf,
+                            cudaStream_t s, ts_dbuf *qbuf) {
+  auto *t = static_cast<ts_tc_tables *>(p->tc);
+  ts_dbuf &b = qbuf ? *qbuf : t->qimg;
+  ensure_zeroed(b, ts_tc_qimg_bytes(p, nf));
+  ts_launch_qimage(p, q, nf, (char *)b.p, s);
+  ts_launch_synth_tc_img(p, (const char *)b.p, nf, fm, fs, s);
+}
+
+void ts_launch_analys_tc_img(ts_plan p, const char *wimg, int nf, float2 *out, long os,
                              cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
@@ -224,12 +361,37 @@ void ts_launch_leg_analys_tc(ts_plan p, const float2 *g, long gs, float2 *out, l
                                  (int)p->ctx->smem_optin));
     attr = true;
   }
-  const TsTcTab &tc = ts_tc_tab(p);
-  dim3 grid((nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS, p->mmax + 1, 2 * ts_tc_ntile(p));
+  const int nfb = (nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS;
+  const int ntile = ts_tc_ntile(p);
+  const int ctas = ts_tc_ctas(p, (long)(p->mmax + 1) * 2 * ntile * nfb);
   TsAnalysStore epi{out, os};
-  ts_leg_analys_tc<TsAnalysStore><<<grid, TS_TC_THREADS, ts_tc_analys_smem(p), s>>>(
-      p->leg, tc, g, gs, epi, nf, TS_TC_FIELDS, ts_tc_analys_stages(p));
+  ts_leg_analys_tc<TsAnalysStore><<<ctas, TS_TC_THREADS, ts_tc_analys_smem(p), s>>>(
+      p->leg, ts_tc_tab(p), wimg, nfb, epi, nf, TS_TC_FIELDS, ts_tc_analys_stages(p),
+      ts_tc_analys_nmax(p), ntile);
   TS_CUDA(cudaGetLastError());
+}
+
+// G (gm layout) -> w image -> q: the stage-level analysis of a TC plan
+void ts_launch_leg_analys_tc(ts_plan p, const float2 *g, long gs, float2 *out, long os, int nf,
+                             cudaStream_t s) {
+  auto *t = static_cast<ts_tc_tables *>(p->tc);
+  ensure_zeroed(t->wimg, ts_tc_wimg_bytes(p, nf, TS_TC_FIELDS));
+  ts_launch_wimage(p, g, gs, nf, TS_TC_FIELDS, (char *)t->wimg.p, s);
+  ts_launch_analys_tc_img(p, (const char *)t->wimg.p, nf, out, os, s);
+}
+
+// spat -> w image directly (register FFT over latitude pairs) when the grid
+// allows it, else spat -> G scratch -> w image; then -> q
+void ts_analys_tc_full(ts_plan p, const float *spat, long ss, float *qlm, int nf, cudaStream_t s) {
+  auto *t = static_cast<ts_tc_tables *>(p->tc);
+  ensure_zeroed(t->wimg, ts_tc_wimg_bytes(p, nf, TS_TC_FIELDS));
+  if (!ts_launch_fourier_analys_w(p, spat, ss, nf, TS_TC_FIELDS, (char *)t->wimg.p, s)) {
+    const long field = (long)(p->mmax + 1) * p->nlat;
+    t->gscratch.ensure(sizeof(float2) * field * nf);
+    ts_launch_fourier_analys(p, spat, ss, (float2 *)t->gscratch.p, field, nf, s);
+    ts_launch_wimage(p, (const float2 *)t->gscratch.p, field, nf, TS_TC_FIELDS, (char *)t->wimg.p, s);
+  }
+  ts_launch_analys_tc_img(p, (const char *)t->wimg.p, nf, (float2 *)qlm, p->nlm, s);
 }
 
 int ts_tc_check_error(ts_plan p) {
