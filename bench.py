@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--precision", default="tf32x3")
     ap.add_argument("--imex-instances", type=int, default=128)
     ap.add_argument("--imex-steps", type=int, default=100)
+    ap.add_argument("--only", choices=["all", "sht", "imex"], default="all",
+                    help="sht: the timed transform pairs alone; imex: the model steps alone "
+                         "(short runs for a profiler's launch list)")
     return ap.parse_args()
 
 
@@ -251,6 +254,68 @@ def time_imex(dev, plan, ninst, K, W, stream):
     return ms, launches, ok
 
 
+def time_e2e(plan, q0, qa, qb, spat, B, K, stream, world, dist):
+    """End to end through the C ABI: every step copies its coefficients from
+    pinned host memory, runs synth + analys and copies the result back.  The
+    copies run on two copy streams (host->device and device->host, full duplex
+    on PCIe) against double-buffered device arrays, so step i's transforms
+    overlap step i+1's upload and step i-1's download, as a serving loop would
+    run them.  Returns (ms for the timed steps, steps, relL2 of the last result)."""
+    import torch
+    hq_in = torch.from_numpy(q0).pin_memory()
+    hq_out = [torch.empty_like(hq_in).pin_memory() for _ in range(2)]
+    d_in = [qa, torch.empty_like(qa)]
+    d_out = [qb, torch.empty_like(qb)]
+    h2d, d2h = torch.cuda.Stream(), torch.cuda.Stream()
+    sp = stream.cuda_stream
+    Ke = max(3, K // 4)
+    loaded = [torch.cuda.Event() for _ in range(2)]
+    computed = [torch.cuda.Event() for _ in range(2)]
+    saved = [torch.cuda.Event() for _ in range(2)]
+
+    def run(n):
+        for i in range(n):
+            j = i & 1
+            if i >= 2:
+                h2d.wait_event(computed[j])        # step i-2 is done reading d_in[j]
+            with torch.cuda.stream(h2d):
+                d_in[j].copy_(hq_in, non_blocking=True)
+                loaded[j].record(h2d)
+            stream.wait_event(loaded[j])
+            if i >= 2:
+                stream.wait_event(saved[j])        # step i-2's result has left d_out[j]
+            plan.synth_dev(d_in[j].data_ptr(), spat.data_ptr(), B, sp)
+            plan.analys_dev(spat.data_ptr(), d_out[j].data_ptr(), B, sp)
+            computed[j].record(stream)
+            d2h.wait_event(computed[j])
+            with torch.cuda.stream(d2h):
+                hq_out[j].copy_(d_out[j], non_blocking=True)
+                saved[j].record(d2h)
+        stream.wait_stream(h2d)
+        stream.wait_stream(d2h)
+
+    run(3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h2d.wait_event(e0)
+    d2h.wait_event(e0)
+    run(Ke)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ems], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    back = hq_out[(Ke - 1) & 1].numpy()
+    err = float(np.sqrt(((back - q0) ** 2).sum() / (q0 ** 2).sum()))
+    return ems, Ke, err
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -284,6 +349,16 @@ def main():
     plain = ShtPlan.create(dev, cfg, {"precision": "fp32"})
     nlm = plan.nlm
 
+    if args.only == "imex":
+        ni = args.imex_instances
+        ims, launches, ok = time_imex(dev, plan, ni, args.imex_steps, max(3, args.warmup), stream)
+        if rank == 0:
+            print(json.dumps({"only": "imex", "instances": ni, "launches_per_step": launches,
+                              "ms_per_step": ims / args.imex_steps, "finite": ok,
+                              "value": world * ni * args.imex_steps / (ims / 1e3),
+                              "unit": "instance-steps/s"}), flush=True)
+        return finish(plan, plain, dev, world)
+
     q0 = np.stack([spectrum(lmax, 1000 * rank + b) for b in range(B)])
     qa = torch.from_numpy(q0).cuda()
     qb = torch.empty_like(qa)
@@ -303,8 +378,9 @@ def main():
 
     K, W = args.steps, max(3, args.warmup)
     # plain FP32 first (untimed by the clock sampler), then the headline path
-    plain_ms, plain_stage = time_round_trips(plain, [qa, qb], spat, fm, B, max(20, K // 4), W,
-                                             stream)
+    if args.only != "sht":
+        plain_ms, plain_stage = time_round_trips(plain, [qa, qb], spat, fm, B, max(20, K // 4),
+                                                 W, stream)
     qa.copy_(torch.from_numpy(q0))
     sampler = ClockSampler(local)
     if world > 1:
@@ -318,30 +394,14 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
 
-    # end to end through the C ABI: pinned host coefficients in, result out, every step
-    hq_in = torch.from_numpy(q0).pin_memory()
-    hq_out = torch.empty_like(hq_in).pin_memory()
-    Ke = max(3, K // 4)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(Ke):
-        qa.copy_(hq_in, non_blocking=True)
-        plan.synth_dev(qa.data_ptr(), spat.data_ptr(), B, sp)
-        plan.analys_dev(spat.data_ptr(), qb.data_ptr(), B, sp)
-        hq_out.copy_(qb, non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ems = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ems], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
-    back = hq_out.numpy()
-    e2e_err = float(np.sqrt(((back - q0) ** 2).sum() / (q0 ** 2).sum()))
+    if args.only == "sht":
+        if rank == 0:
+            print(json.dumps({"only": "sht", "ms_per_step": ms / K, "stage_ms": stage_ms,
+                              "value": world * B * K / (ms / 1e3), "unit": "SHT pairs/s"}),
+                  flush=True)
+        return finish(plan, plain, dev, world)
+
+    ems, Ke, e2e_err = time_e2e(plan, q0, qa, qb, spat, B, K, stream, world, dist)
 
     # IMEX steps: batched Schnakenberg instances on the same grid, both precisions
     del spat, fm
@@ -409,10 +469,15 @@ def main():
         line["imex"]["tc_vs_fp32"] = line["imex"]["tc_steps_per_s"] / line["imex"]["fp32_steps_per_s"]
         line["tc_vs_plain_sht"] = value / line["plain_fp32"]["value"]
         print(json.dumps(line), flush=True)
+    return finish(plan, plain, dev, world)
+
+
+def finish(plan, plain, dev, world):
     plan.destroy()
     plain.destroy()
     dev.destroy()
     if world > 1:
+        import torch.distributed as dist
         dist.destroy_process_group()
     return 0
 

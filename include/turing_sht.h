@@ -55,6 +55,7 @@ enum ts_plan_flags {
   TS_PREC_TF32X3 = 1,      /* tcgen05 tensor-core Legendre, 3-pass split TF32 */
   TS_PREC_BF16X3 = 2,      /* tcgen05 tensor-core Legendre, 3-pass split BF16 */
   TS_PREC_MASK = 0xF,
+  TS_CHECK_SOURCE = 0x100, /* ts_model_check: return the generated source */
   TS_FOURIER_AUTO = 0,     /* mixed-radix FFT whenever nphi = 2^a 3^b, else DFT */
   TS_FOURIER_FFT = 0x10,   /* require the FFT (error if nphi has other factors) */
   TS_FOURIER_DFT = 0x20,   /* direct band-limited sum (sht.ts:241-289 semantics) */
@@ -219,8 +220,10 @@ int ts_model_counts(ts_model model, int which, int *kernels, int *launches);
  * schedule, generate CUDA C and compile it with NVRTC for sm_100a — for a grid
  * given by its sizes (no context, no device).  `describe` receives the
  * describe() text of init and step separated by a "====" line; flags selects
- * the precision (TS_PREC_*) whose kernels are generated; `kernels` and
- * `launches` are those of step.  For host-side checks of a model source
+ * the precision (TS_PREC_*) whose kernels are generated, optionally ORed
+ * with TS_CHECK_SOURCE to receive the generated CUDA source of both programs
+ * in `describe` instead of the stage list; `kernels` and `launches` are those
+ * of step.  For host-side checks of a model source
  * (the editor's compile-on-type, src/editor/, and the tests). */
 int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
                    const char *const *state, int nstate, const char *const *view, int nview,

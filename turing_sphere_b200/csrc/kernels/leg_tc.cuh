@@ -196,7 +196,24 @@ struct TsTcPipe {
   unsigned long long drain;  // the MMA warp's last commit before exit
   unsigned tmem;
   int bad;
+  int epi_go[2];  // per accumulator buffer: the epilogue warps proceed (1) or leave (0)
 };
+
+// shared-memory staging of the epilogues: the synthesis keeps 64 field rows
+// of [north|south][16 latitudes][re, im] (68 floats per row keeps rows
+// 16-byte aligned); the analysis keeps [l][re|im] rows of 64 fields padded to
+// 65 floats, so that lanes reading different rows hit different banks
+#define TS_TC_SYN_ROW 68
+#define TS_TC_SYN_STAGING (TS_TC_FIELDS * TS_TC_SYN_ROW * 4)
+#define TS_TC_ANA_ROW (TS_TC_FIELDS + 1)
+
+// barrier of the 4 epilogue warps (named barrier 1).  Every epilogue warp
+// runs the same sequence of these (exits are decided uniformly, through
+// TsTcPipe::epi_go), so none is left waiting.
+TS_DEV void ts_epi_bar() {
+  __syncwarp();
+  asm volatile("bar.sync 1, 128;" ::: "memory");
+}
 
 TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S) {
   if (threadIdx.x == 0) {
@@ -371,19 +388,20 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
       if (!ts_mbar_wait(&pp->drain, 0, TS_TC_WAIT_LIMIT)) ts_tc_flag(pp);
     }
   } else {
+    // one thread waits for the accumulator and tells the other epilogue warps
+    // whether to go on, so that they all take the same barriers
     int i = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
       const int b = i & 1;
-      const bool ok = ts_mbar_wait(&pp->acc_full[b], (i >> 1) & 1, TS_TC_WAIT_LIMIT);
-      if (!ok || ts_tc_bad(pp)) {
-        ts_tc_flag(pp);
-        return;
+      if (warp == 6 && lane == 0) {
+        const bool ok = ts_mbar_wait(&pp->acc_full[b], (i >> 1) & 1, TS_TC_WAIT_LIMIT);
+        if (!ok) ts_tc_flag(pp);
+        pp->epi_go[b] = ok && !ts_tc_bad(pp);
       }
+      ts_epi_bar();
+      if (!*reinterpret_cast<volatile int *>(&pp->epi_go[b])) return;
       ts_tc_fence_after();
-      if (!epilogue(tile, tmem + (unsigned)(b * acc_cols))) {
-        ts_tc_flag(pp);
-        return;
-      }
+      epilogue(tile, tmem + (unsigned)(b * acc_cols));
       ts_tc_fence_before();
       __syncwarp();
       if (lane == 0) ts_mbar_arrive(&pp->acc_empty[b]);
@@ -393,15 +411,6 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
 
 // rows 32*(warp%4) .. of TMEM belong to epilogue warp `warp` (warps 6-9)
 TS_DEV int ts_epi_row(int warp, int lane) { return (warp & 3) * 32 + lane; }
-
-// barrier of the 4 epilogue warps, bounded; `phase` counts its uses
-TS_DEV bool ts_epi_sync(TsTcPipe *pp, unsigned &phase) {
-  __syncwarp();
-  if ((threadIdx.x & 31) == 0) ts_mbar_arrive(&pp->epi);
-  const bool ok = ts_mbar_wait(&pp->epi, phase & 1, TS_TC_WAIT_LIMIT);
-  phase++;
-  return ok;
-}
 
 // ----------------------------------------------------------------- synthesis
 struct TsSynthSched {
@@ -469,7 +478,8 @@ struct TsSynthSched {
 };
 
 // grid = min(#SMs, tiles), block = 320, persistent.  Dynamic shared memory:
-// S*(2*16384 + 2*NL*128) + 1024 + sizeof(TsTcPipe).  TMEM: two buffers of 2*NL.
+// S*(2*16384 + 2*NL*128) + TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe).
+// TMEM: two buffers of 2*NL columns.
 __global__ void __launch_bounds__(TS_TC_THREADS, 1)
 ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb,
                 float2 *__restrict__ fm, long fm_stride, int nfields, int S) {
@@ -478,7 +488,7 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
   const int NL = tc.NL;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned stage = 2 * 16384 + 2 * NL * 128;
-  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage);
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + TS_TC_SYN_STAGING);
   const TsSynthSched sc{&tc, t.lmax, t.mmax, q_nfb, NL, tc.nLT, qimg};
   ts_tc_pipe_init(pp, S);
   if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
@@ -487,17 +497,19 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
   ts_tc_fence_after();
   const unsigned tmem = pp->tmem;
 
-  // epilogue: rows 2f (re) and 2f+1 (im) sit in adjacent lanes; each pair
-  // swaps halves so that every thread writes 8 consecutive complex values,
-  // north and (mirrored) south
-  auto epilogue = [&](int tile, unsigned tbase) -> bool {
+  // epilogue, per 16 latitudes: each thread (row 2f+re|im) puts north = E+O
+  // and south = E-O of its component into the staging rows; then the 128
+  // threads write 16-byte runs of whole complex values, north in latitude
+  // order and south mirrored, 8 lanes covering one field's 128-byte run
+  float *sE = reinterpret_cast<float *>(smem + S * stage);
+  const bool vec = (t.nlat % 2 == 0) && (fm_stride % 2 == 0) &&
+                   ((reinterpret_cast<unsigned long long>(fm) & 15) == 0);
+  auto epilogue = [&](int tile, unsigned tbase) {
     int m, lt, fb, n0, n1;
     sc.decode(tile, m, lt, fb);
     sc.nch(m, n0, n1);
-    const int row = ts_epi_row(warp, lane);
-    const int fl = row >> 1, comp = lane & 1;
-    const int f = fb * TS_TC_FIELDS + fl;
-    float2 *dst = fm + (long)f * fm_stride + (long)m * t.nlat;
+    const int et = ts_epi_row(warp, lane);  // 0..127 = TMEM lane = 2*field + comp
+    float *mine = sE + (et >> 1) * TS_TC_SYN_ROW + (et & 1);
     const unsigned lanebase = tbase + ((unsigned)((warp & 3) * 32) << 16);
     for (int c0 = 0; c0 < NL; c0 += 16) {
       float e[16], o[16];
@@ -507,27 +519,42 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
       else
 #pragma unroll
         for (int i = 0; i < 16; i++) o[i] = 0.f;
-      float2 en[8], on[8];
 #pragma unroll
-      for (int i = 0; i < 8; i++) {
-        const float se = __shfl_xor_sync(0xffffffffu, comp ? e[i] : e[8 + i], 1);
-        const float so = __shfl_xor_sync(0xffffffffu, comp ? o[i] : o[8 + i], 1);
-        en[i] = comp ? make_float2(se, e[8 + i]) : make_float2(e[i], se);
-        on[i] = comp ? make_float2(so, o[8 + i]) : make_float2(o[i], so);
+      for (int i = 0; i < 16; i++) {
+        mine[2 * i] = e[i] + o[i];
+        mine[32 + 2 * i] = e[i] - o[i];
       }
-      if (f < nfields) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-          const int lat = lt * NL + c0 + comp * 8 + i;
-          if (lat < t.nh) {
-            dst[lat] = make_float2(en[i].x + on[i].x, en[i].y + on[i].y);
-            const int south = t.nlat - 1 - lat;
-            if (south != lat) dst[south] = make_float2(en[i].x - on[i].x, en[i].y - on[i].y);
+      ts_epi_bar();
+#pragma unroll 2
+      for (int k = 0; k < 8; k++) {
+        const int q = et + 128 * k, seg = q >> 3, part = q & 7;
+        const int fl = seg >> 1, ns = seg & 1;
+        const float4 v =
+            *reinterpret_cast<const float4 *>(sE + fl * TS_TC_SYN_ROW + ns * 32 + part * 4);
+        const int f = fb * TS_TC_FIELDS + fl;
+        const int lat = lt * NL + c0 + 2 * part;
+        if (f >= nfields || lat >= t.nh) continue;
+        float2 *row = fm + (long)f * fm_stride + (long)m * t.nlat;
+        const bool two = lat + 1 < t.nh;
+        if (ns == 0) {
+          if (vec && two) {
+            *reinterpret_cast<float4 *>(row + lat) = v;
+          } else {
+            row[lat] = make_float2(v.x, v.y);
+            if (two) row[lat + 1] = make_float2(v.z, v.w);
+          }
+        } else {
+          const int s0 = t.nlat - 1 - lat, s1 = s0 - 1;  // south of lat, lat + 1
+          if (vec && two) {
+            *reinterpret_cast<float4 *>(row + s1) = make_float4(v.z, v.w, v.x, v.y);
+          } else {
+            if (s0 != lat) row[s0] = make_float2(v.x, v.y);
+            if (two && s1 != lat + 1) row[s1] = make_float2(v.z, v.w);
           }
         }
       }
+      ts_epi_bar();
     }
-    return true;
   };
   ts_tc_persistent(smem, pp, S, stage, tmem, 2 * NL, sc, epilogue);
   ts_tc_fence_before();
@@ -574,7 +601,7 @@ struct TsAnalysSched {
 
 // grid = min(#SMs, tiles), block = 320, persistent.  Tiles with no l values
 // have no stages; their epilogue does nothing.  Dynamic shared memory:
-// S*(2*16384 + 2*Nmax*128) + Nmax*2*64*4 + 1024 + sizeof(TsTcPipe).  TMEM:
+// S*(2*16384 + 2*Nmax*128) + Nmax*2*TS_TC_ANA_ROW*4 + 1024 + sizeof(TsTcPipe).  TMEM:
 // two buffers of 256 columns.
 template <class Epi>
 __global__ void __launch_bounds__(TS_TC_THREADS, 1)
@@ -585,7 +612,7 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned stage = 2 * 16384 + 2 * nmax * 128;
   float *sD = reinterpret_cast<float *>(smem + S * stage);
-  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + nmax * 2 * TS_TC_FIELDS * 4);
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + nmax * 2 * TS_TC_ANA_ROW * 4);
   const TsAnalysSched sc{&tc, t.lmax, t.mmax, w_nfb, ntile, wimg};
   ts_tc_pipe_init(pp, S);
   if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
@@ -595,32 +622,30 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
   const unsigned tmem = pp->tmem;
 
   // epilogue: TMEM -> shared [j][comp][field] -> Epi per (lm, comp)
-  unsigned ephase = 0;
-  auto epilogue = [&](int tile, unsigned tbase) -> bool {
+  auto epilogue = [&](int tile, unsigned tbase) {
     const int cnt = sc.cnt(tile);
-    if (cnt == 0) return true;
+    if (cnt == 0) return;
     int m, par, lt, fb;
     sc.decode(tile, m, par, lt, fb);
     const int N = ts_round16(cnt);
     const int row = ts_epi_row(warp, lane), fl = row >> 1, comp = row & 1;
     const unsigned lanebase = tbase + ((unsigned)((warp & 3) * 32) << 16);
-    if (!ts_epi_sync(pp, ephase)) return false;  // the previous tile's epi calls are done with sD
+    ts_epi_bar();  // the previous tile's epi calls are done with sD
     for (int c0 = 0; c0 < N; c0 += 16) {
       float v[16];
       ts_tmem_ld16(lanebase + (unsigned)c0, v);
 #pragma unroll
-      for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_FIELDS + fl] = v[i];
+      for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_ANA_ROW + fl] = v[i];
     }
-    if (!ts_epi_sync(pp, ephase)) return false;
+    ts_epi_bar();
     const int f0 = fb * per_cta;
     const int nf = min(per_cta, nfields - f0);
     const long base = ts_lm_base(t.lmax, m);
     for (int idx = (warp & 3) * 32 + lane; idx < cnt * 2; idx += 128) {
       const int j = idx >> 1, cp = idx & 1;
       const int l = m + par + 2 * (lt * tc.LTL + j);
-      epi(base + (l - m), cp, sD + (j * 2 + cp) * TS_TC_FIELDS, f0, nf, TS_TC_FIELDS);
+      epi(base + (l - m), cp, sD + (j * 2 + cp) * TS_TC_ANA_ROW, f0, nf, TS_TC_FIELDS);
     }
-    return true;
   };
   ts_tc_persistent(smem, pp, S, stage, tmem, 256, sc, epilogue);
   ts_tc_fence_before();

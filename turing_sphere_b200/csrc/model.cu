@@ -482,41 +482,58 @@ void schedule(ts_model m, Program &P, bool is_step) {
     Emitter em{f, {}};
     const std::string en = "TsEpi_" + ptag + std::to_string(tag++);
     std::ostringstream src;
+    // The state inputs of 8 instances are loaded before any of their stores:
+    // the loads then overlap instead of each waiting out the previous store
+    // (the restrict-qualified locals tell the compiler that they do not alias).
+    const int NA = (int)A.size();
     src << "struct " << en << " {\n  TsSpecIO io;\n"
         << "  __device__ __forceinline__ void operator()(long lm, int comp, const float *vals, "
            "int f0, int nf, int F) const {\n"
         << "    const long idx = 2 * lm + comp;\n"
-        << "    for (int i = 0; i < nf / " << A.size() << "; i++) {\n"
-        << "      const long inst = f0 / " << A.size() << " + i;\n"
-        << "      const float *prm = io.prm + inst * io.nprm;\n";
+        << "    const int ni = nf / " << NA << ";\n";
+    for (size_t k = 0; k < sin.size(); k++)
+      src << "    const float *__restrict__ in" << k << " = io.sin[" << k << "];\n";
+    for (size_t o = 0; o < sout.size(); o++)
+      src << "    float *__restrict__ out" << o << " = io.sout[" << o << "];\n";
+    src << "    for (int i0 = 0; i0 < ni; i0 += 8) {\n";
+    for (size_t k = 0; k < sin.size(); k++) src << "      float ld" << k << "[8];\n";
+    src << "#pragma unroll\n      for (int u = 0; u < 8; u++) {\n"
+        << "        if (i0 + u >= ni) break;\n"
+        << "        const long inst = f0 / " << NA << " + i0 + u;\n";
+    for (size_t k = 0; k < sin.size(); k++)
+      src << "        ld" << k << "[u] = in" << k << "[inst * io.sin_stride[" << k << "] + idx];\n";
+    src << "      }\n#pragma unroll\n      for (int u = 0; u < 8; u++) {\n"
+        << "        if (i0 + u >= ni) break;\n"
+        << "        const int i = i0 + u;\n"
+        << "        const long inst = f0 / " << NA << " + i;\n"
+        << "        const float *__restrict__ prm = io.prm + inst * io.nprm;\n";
     {
       std::istringstream sc(em.scalars());
       std::string line;
-      while (std::getline(sc, line)) src << "    " << line << "\n";
+      while (std::getline(sc, line)) src << "      " << line << "\n";
     }
     for (size_t a = 0; a < A.size(); a++) {
       const int v = f.body[A[a]].out;
-      src << "      const float v" << v << " = vals[i * " << A.size() << " + " << a << "];  // "
+      src << "        const float v" << v << " = vals[i * " << NA << " + " << a << "];  // "
           << f.vars[v].name << "\n";
       em.name[v] = "v" + std::to_string(v);
     }
     int k = 0;
     for (int v : sin) {
-      src << "      const float v" << v << " = io.sin[" << k << "][inst * io.sin_stride[" << k
-          << "] + idx];  // " << f.vars[v].name << "\n";
+      src << "        const float v" << v << " = ld" << k << "[u];  // " << f.vars[v].name << "\n";
       em.name[v] = "v" + std::to_string(v);
       k++;
     }
     for (int i : E) {
       const auto &s = f.body[i];
-      src << "      const float v" << s.out << " = " << em.e(s.expr) << ";  // "
+      src << "        const float v" << s.out << " = " << em.e(s.expr) << ";  // "
           << f.vars[s.out].name << "\n";
       em.name[s.out] = "v" + std::to_string(s.out);
     }
     for (size_t o = 0; o < sout.size(); o++)
-      src << "      io.sout[" << o << "][inst * io.sout_stride[" << o << "] + idx] = v"
-          << sout[o] << ";\n";
-    src << "    }\n  }\n};\n";
+      src << "        out" << o << "[inst * io.sout_stride[" << o << "] + idx] = v" << sout[o]
+          << ";\n";
+    src << "      }\n    }\n  }\n};\n";
     st.expr = tc ? "ts_leg_analys_tc<" + en + ">"
                  : "ts_leg_analys_f32<" + std::to_string(st.F) + ", " + std::to_string(st.K) +
                        ", 2, " + en + ">";
@@ -1159,9 +1176,15 @@ int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
     finish_shapes(&mod);
     std::map<std::string, std::string> lowered;
     build_cubin(&mod, lowered);
-    if (describe && cap)
+    if (describe && cap && (flags & TS_CHECK_SOURCE)) {
+      std::string code;
+      for (auto &P : mod.prog)
+        for (auto &st : P.stages) code += stage_source(st);
+      snprintf(describe, cap, "%s", code.c_str());
+    } else if (describe && cap) {
       snprintf(describe, cap, "%s====\n%s", describe_program(mod.prog[0]).c_str(),
                describe_program(mod.prog[1]).c_str());
+    }
     if (kernels) *kernels = tsm::count_kernels(mod.prog[1].fn);
     if (launches) *launches = (int)mod.prog[1].stages.size();
     return TS_OK;
