@@ -1,0 +1,516 @@
+// Longitude stage on a two-phase shared-memory FFT.
+//
+// The real-row conventions are those of fourier.cuh: a row of nphi real
+// values is a half-length complex row z[n] = x[2n] + i x[2n+1] of H = nphi/2
+// points, and
+//   synthesis: Z[k] = (X[k] + conj X[H-k]) + i e^{+2 pi i k/nphi} (X[k] - conj X[H-k]),
+//              z = FFT_H^{+}(Z);
+//   analysis:  Z = FFT_H^{-}(z),
+//              X[k] = (Z[k] + conj Z[H-k])/2 - i e^{-2 pi i k/nphi} (Z[k] - conj Z[H-k])/2.
+//
+// A CTA holds R rows in shared memory and transforms them in place, with
+// H = P * Q split as (w = e^{2 pi i/H})
+//   k = k1 + P k2,  n = Q n1 + n2   (k1, n1 < P;  k2, n2 < Q)
+//   z[Q n1 + n2] = sum_k1 e^{2 pi i n1 k1/P} w^{n2 k1} sum_k2 Z[k1 + P k2] e^{2 pi i n2 k2/Q}.
+// Phase 1 gives every thread one (row, k1) and a Q-point DFT in registers;
+// phase 2 one (row, n2) and a P-point DFT.  The analysis runs the mirror
+// image (P-point DFTs, conjugate twiddles, Q-point DFTs).  Between the
+// phases a row is stored transposed, element (k1, n2) at n2 (P+1) + k1; with
+// P even the odd pitch P+1, and an odd row pitch, make every phase's shared
+// accesses conflict-free (lanes step through consecutive k1, n2 or rows).
+// The DFTs inside a thread are Stockham sequences over compile-time radices
+// (4, 2, 3) whose twiddles are compile-time constants.
+//
+// Global traffic: spectra are read and written as fm[m][lat] with
+// consecutive threads on consecutive latitudes; grid rows as whole rows.
+#pragma once
+#include "ts_common.cuh"
+
+// ------------------------------------------------- compile-time helpers
+template <int V>
+struct TsIC {
+  static constexpr int value = V;
+};
+
+// f(TsIC<B>{}), f(TsIC<B+1>{}), ..., f(TsIC<E-1>{})
+template <int B, int E, class F>
+TS_DEV void ts_sfor(F &&f) {
+  if constexpr (B < E) {
+    f(TsIC<B>{});
+    ts_sfor<B + 1, E>(f);
+  }
+}
+
+// cos and sin of 2 pi num/den, evaluated by the compiler: the angle is
+// reduced to [-pi, pi] exactly (integer arithmetic) and summed as a Taylor
+// series in double precision (16 terms: remainder below 1e-18 at |x| = pi).
+constexpr double ts_cx_pi = 3.14159265358979323846264338327950288;
+__host__ __device__ constexpr double ts_cx_angle(long num, long den) {
+  long n = num % den;
+  if (n < 0) n += den;
+  if (2 * n > den) n -= den;
+  return 2.0 * ts_cx_pi * (double)n / (double)den;
+}
+__host__ __device__ constexpr double ts_cx_sin_series(double x) {
+  double t = x, s = x;
+  for (int i = 1; i < 16; i++) {
+    t *= -x * x / ((2.0 * i) * (2.0 * i + 1.0));
+    s += t;
+  }
+  return s;
+}
+__host__ __device__ constexpr double ts_cx_cos_series(double x) {
+  double t = 1.0, s = 1.0;
+  for (int i = 1; i < 16; i++) {
+    t *= -x * x / ((2.0 * i - 1.0) * (2.0 * i));
+    s += t;
+  }
+  return s;
+}
+__host__ __device__ constexpr float ts_cx_cos(long num, long den) { return (float)ts_cx_cos_series(ts_cx_angle(num, den)); }
+__host__ __device__ constexpr float ts_cx_sin(long num, long den) { return (float)ts_cx_sin_series(ts_cx_angle(num, den)); }
+
+// a * e^{SIGN 2 pi i NUM/DEN}; quarter turns are exact swaps and negations
+template <long NUM, long DEN, int SIGN>
+TS_DEV float2 ts_twc(float2 a) {
+  constexpr long n = ((NUM % DEN) + DEN) % DEN;
+  if constexpr (n == 0) {
+    return a;
+  } else if constexpr (2 * n == DEN) {
+    return make_float2(-a.x, -a.y);
+  } else if constexpr (4 * n == DEN) {
+    return SIGN > 0 ? c_mul_i(a) : c_mul_negi(a);
+  } else if constexpr (4 * n == 3 * DEN) {
+    return SIGN > 0 ? c_mul_negi(a) : c_mul_i(a);
+  } else {
+    constexpr float c = ts_cx_cos(n, DEN);
+    constexpr float s = SIGN * ts_cx_sin(n, DEN);
+    return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+  }
+}
+
+template <int M>
+struct TsRadix {
+  static constexpr int value = (M % 4 == 0) ? 4 : (M % 2 == 0) ? 2 : 3;
+};
+
+// R-point DFT (R = 2, 3, 4) of a[0..R), sign SIGN
+template <int R, int SIGN>
+TS_DEV void ts_butterfly(float2 (&a)[R]) {
+  if constexpr (R == 2) {
+    const float2 s = c_add(a[0], a[1]), d = c_sub(a[0], a[1]);
+    a[0] = s;
+    a[1] = d;
+  } else if constexpr (R == 3) {
+    const float2 s12 = c_add(a[1], a[2]);
+    const float2 d12 = c_sub(a[1], a[2]);
+    const float2 mid = make_float2(a[0].x - 0.5f * s12.x, a[0].y - 0.5f * s12.y);
+    const float h = SIGN * 0.8660254037844386f;  // sin(2 pi/3)
+    const float2 rot = make_float2(-h * d12.y, h * d12.x);
+    a[0] = c_add(a[0], s12);
+    a[1] = c_add(mid, rot);
+    a[2] = c_sub(mid, rot);
+  } else if constexpr (R == 4) {
+    const float2 p = c_add(a[0], a[2]), q = c_sub(a[0], a[2]);
+    const float2 r = c_add(a[1], a[3]), e = c_sub(a[1], a[3]);
+    const float2 d = SIGN > 0 ? c_mul_i(e) : c_mul_negi(e);
+    a[0] = c_add(p, r);
+    a[1] = c_add(q, d);
+    a[2] = c_sub(p, r);
+    a[3] = c_sub(q, d);
+  }
+}
+
+// Stockham stage NS of an N-point DFT in registers, then the remaining ones
+template <int N, int NS, int SIGN>
+TS_DEV void ts_dft_rec(float2 (&x)[N]) {
+  if constexpr (NS < N) {
+    constexpr int R = TsRadix<N / NS>::value;
+    constexpr int MR = N / R;
+    float2 y[N];
+    ts_sfor<0, MR>([&](auto tc) {
+      constexpr int t = decltype(tc)::value;
+      constexpr int j = t % NS;
+      float2 a[R];
+      ts_sfor<0, R>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        a[q] = ts_twc<(long)q * j, (long)NS * R, SIGN>(x[t + q * MR]);
+      });
+      ts_butterfly<R, SIGN>(a);
+      ts_sfor<0, R>([&](auto qc) {
+        constexpr int q = decltype(qc)::value;
+        y[(t - j) * R + j + q * NS] = a[q];
+      });
+    });
+#pragma unroll
+    for (int i = 0; i < N; i++) x[i] = y[i];
+    ts_dft_rec<N, NS * R, SIGN>(x);
+  }
+}
+
+// N-point DFT, natural order in and out: x[k] <- sum_n x[n] e^{SIGN 2 pi i nk/N}
+template <int N, int SIGN>
+TS_DEV void ts_dft(float2 (&x)[N]) {
+  ts_dft_rec<N, 1, SIGN>(x);
+}
+
+// ------------------------------------------------------------- geometry
+template <int P_, int Q_, int R_>
+struct TsF2 {
+  static constexpr int P = P_, Q = Q_, R = R_, H = P_ * Q_, T = P_ * R_;
+  static constexpr int P1 = P_ + 1;        // pitch of the transposed view
+  static constexpr int RP = (H + Q_) | 1;  // row pitch: odd, >= Q (P+1) = H + Q
+  static constexpr int TWQ = Q_ * P1;      // inter-phase twiddles [n2][k1]
+};
+
+// twq[n2 (P+1) + k1] = w^{n2 k1}
+template <class C>
+TS_DEV void ts_f2_twq(float2 *twq, const TsFftTab &ft) {
+  for (int i = threadIdx.x; i < C::Q * C::P; i += C::T) {
+    const int n2 = i / C::P, k1 = i - n2 * C::P;
+    twq[n2 * C::P1 + k1] = __ldg(ft.tw + (2 * n2 * k1) % ft.nphi);
+  }
+}
+
+// z = FFT_H^{+}(Z) of the R rows at b (natural order in and out)
+template <class C>
+TS_DEV void ts_f2_inverse(float2 *b, const float2 *twq) {
+  const int tid = threadIdx.x;
+  {
+    const int r = tid / C::P, k1 = tid - r * C::P;
+    float2 *row = b + r * C::RP;
+    float2 x[C::Q];
+#pragma unroll
+    for (int k2 = 0; k2 < C::Q; k2++) x[k2] = row[k1 + C::P * k2];
+    ts_dft<C::Q, +1>(x);
+#pragma unroll
+    for (int n2 = 1; n2 < C::Q; n2++) x[n2] = c_mul(x[n2], twq[n2 * C::P1 + k1]);
+    __syncthreads();
+#pragma unroll
+    for (int n2 = 0; n2 < C::Q; n2++) row[n2 * C::P1 + k1] = x[n2];
+    __syncthreads();
+  }
+  {
+    const bool act = tid < C::Q * C::R;
+    const int r = tid / C::Q, n2 = tid - r * C::Q;
+    float2 *row = b + r * C::RP;
+    float2 x[C::P];
+    if (act) {
+#pragma unroll
+      for (int k1 = 0; k1 < C::P; k1++) x[k1] = row[n2 * C::P1 + k1];
+      ts_dft<C::P, +1>(x);
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int n1 = 0; n1 < C::P; n1++) row[C::Q * n1 + n2] = x[n1];
+    }
+    __syncthreads();
+  }
+}
+
+// Z = FFT_H^{-}(z) of the R rows at b (natural order in and out)
+template <class C>
+TS_DEV void ts_f2_forward(float2 *b, const float2 *twq) {
+  const int tid = threadIdx.x;
+  {
+    const bool act = tid < C::Q * C::R;
+    const int r = tid / C::Q, n2 = tid - r * C::Q;
+    float2 *row = b + r * C::RP;
+    float2 x[C::P];
+    if (act) {
+#pragma unroll
+      for (int n1 = 0; n1 < C::P; n1++) x[n1] = row[C::Q * n1 + n2];
+      ts_dft<C::P, -1>(x);
+#pragma unroll
+      for (int k1 = 1; k1 < C::P; k1++) x[k1] = c_mul(x[k1], c_conj(twq[n2 * C::P1 + k1]));
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int k1 = 0; k1 < C::P; k1++) row[n2 * C::P1 + k1] = x[k1];
+    }
+    __syncthreads();
+  }
+  {
+    const int r = tid / C::P, k1 = tid - r * C::P;
+    float2 *row = b + r * C::RP;
+    float2 x[C::Q];
+#pragma unroll
+    for (int n2 = 0; n2 < C::Q; n2++) x[n2] = row[n2 * C::P1 + k1];
+    ts_dft<C::Q, -1>(x);
+    __syncthreads();
+#pragma unroll
+    for (int k2 = 0; k2 < C::Q; k2++) row[k1 + C::P * k2] = x[k2];
+    __syncthreads();
+  }
+}
+
+// Z of the synthesis for the CTA's rows from the spectra src[k*nlat + lat]
+// of one field.  lat_of(r) < 0 marks a row without a latitude (zeros).
+// Thread i takes the pair (k, H-k), k = i / R, of row i % R: consecutive
+// threads read consecutive latitudes.
+template <class C, class LatOf>
+TS_DEV void ts_f2_pack(float2 *b, const float2 *__restrict__ src, const TsFftTab &ft,
+                       LatOf lat_of) {
+  constexpr int H = C::H, NK = H / 2 + 1;
+  for (int i = threadIdx.x; i < NK * C::R; i += C::T) {
+    const int kk = i / C::R, r = i - kk * C::R;
+    const int h = H - kk;
+    const int lat = lat_of(r);
+    float2 xk = make_float2(0.f, 0.f), xh = make_float2(0.f, 0.f);
+    if (lat >= 0) {
+      if (kk <= ft.mmax) {
+        xk = src[(long)kk * ft.nlat + lat];
+        if (kk == 0) xk.y = 0.f;
+      }
+      if (h <= ft.mmax) xh = src[(long)h * ft.nlat + lat];
+    }
+    float2 *row = b + r * C::RP;
+    const float2 ch = c_conj(xh);
+    row[kk] = c_add(c_add(xk, ch), c_mul_i(c_mul(c_sub(xk, ch), __ldg(ft.tw + kk))));
+    if (kk > 0 && kk < h) {
+      const float2 ck = c_conj(xk);
+      row[h] = c_add(c_add(xh, ck), c_mul_i(c_mul(c_sub(xh, ck), __ldg(ft.tw + h))));
+    }
+  }
+}
+
+// X[k] of the analysis from the forward-transformed row
+template <class C>
+TS_DEV float2 ts_f2_xk(const float2 *row, int k, const TsFftTab &ft) {
+  const float2 zk = row[k];
+  const float2 zh = c_conj(row[k == 0 ? 0 : C::H - k]);
+  const float2 xe = c_scale(c_add(zk, zh), 0.5f);
+  const float2 xo = c_mul_negi(c_scale(c_sub(zk, zh), 0.5f));
+  return c_add(xe, c_mul(xo, c_conj(__ldg(ft.tw + k))));
+}
+
+// X[k], k <= mmax, of the CTA's rows -> dst[k*nlat + lat]
+template <class C, class LatOf>
+TS_DEV void ts_f2_unpack(const float2 *b, float2 *__restrict__ dst, const TsFftTab &ft,
+                         LatOf lat_of) {
+  const int n = (ft.mmax + 1) * C::R;
+  for (int i = threadIdx.x; i < n; i += C::T) {
+    const int k = i / C::R, r = i - k * C::R;
+    const int lat = lat_of(r);
+    if (lat >= 0) dst[(long)k * ft.nlat + lat] = ts_f2_xk<C>(b + r * C::RP, k, ft);
+  }
+}
+
+// grid rows: b <-> rows of src/dst (row `lat` starts at lat*nphi floats)
+template <class C, class LatOf>
+TS_DEV void ts_f2_load_rows(float2 *b, const float *__restrict__ src, int nphi, LatOf lat_of) {
+  for (int i = threadIdx.x; i < C::R * C::H; i += C::T) {
+    const int r = i / C::H, n = i - r * C::H;
+    const int lat = lat_of(r);
+    b[r * C::RP + n] = lat >= 0 ? reinterpret_cast<const float2 *>(src + (long)lat * nphi)[n]
+                                : make_float2(0.f, 0.f);
+  }
+}
+
+template <class C, class LatOf>
+TS_DEV void ts_f2_store_rows(const float2 *b, float *__restrict__ dst, int nphi, LatOf lat_of) {
+  for (int i = threadIdx.x; i < C::R * C::H; i += C::T) {
+    const int r = i / C::H, n = i - r * C::H;
+    const int lat = lat_of(r);
+    if (lat >= 0) reinterpret_cast<float2 *>(dst + (long)lat * nphi)[n] = b[r * C::RP + n];
+  }
+}
+
+// ------------------------------------------------- W image of the TC path
+//
+// Tensor-core plans consume the analysis as W_par = w (G_north +- G_south)
+// in the MMA's byte image (TsTcImg.w).  A paired CTA holds R/2 northern
+// latitudes lat0 + j in rows j and their southern mirrors in rows R/2 + j
+// (a row without a latitude, or the equator's repeat, reads as zero), and
+// writes the folded, weighted values: with R/2 = 8 and lat0 a multiple of 8,
+// every (m, parity, re|im) run covers one whole 32-byte sector of the image.
+template <class C>
+TS_DEV void ts_f2_write_w(const float2 *b, int lat0, long f, const TsFftTab &ft,
+                          const float *__restrict__ wq, char *wimg, int nfb, int fpb, int nlc,
+                          int nh) {
+  constexpr int NPR = C::R / 2;
+  const long fb = f / fpb;
+  const int fl = (int)(f - fb * fpb);
+  const int n = (ft.mmax + 1) * NPR;
+  for (int i = threadIdx.x; i < n; i += C::T) {
+    const int k = i / NPR, j = i - k * NPR;
+    const int lat = lat0 + j;
+    if (lat >= nh) continue;
+    const float2 xn = ts_f2_xk<C>(b + j * C::RP, k, ft);
+    const float2 xs = (ft.nlat - 1 - lat != lat) ? ts_f2_xk<C>(b + (NPR + j) * C::RP, k, ft)
+                                                 : make_float2(0.f, 0.f);
+    const float w = __ldg(wq + lat);
+#pragma unroll
+    for (int par = 0; par < 2; par++) {
+      const long blk = (((long)k * nfb + fb) * 2 + par) * nlc + (lat >> 5);
+      char *base = wimg + blk * 16384;
+      const float re = w * (par ? xn.x - xs.x : xn.x + xs.x);
+      const float im = w * (par ? xn.y - xs.y : xn.y + xs.y);
+      *reinterpret_cast<float *>(base + ts_swz_img(2 * fl, lat & 31)) = re;
+      *reinterpret_cast<float *>(base + ts_swz_img(2 * fl + 1, lat & 31)) = im;
+    }
+  }
+}
+
+// latitude of row r: plain CTAs hold lat0 + r; paired CTAs northern rows
+// lat0 + r (r < R/2) and their mirrors
+template <class C, bool PAIRED>
+struct TsF2Rows {
+  int lat0, nlat, nh;
+  TS_DEV int operator()(int r) const {
+    if constexpr (PAIRED) {
+      const int j = r < C::R / 2 ? r : r - C::R / 2;
+      const int latN = lat0 + j;
+      if (latN >= nh) return -1;
+      if (r < C::R / 2) return latN;
+      const int latS = nlat - 1 - latN;
+      return latS != latN ? latS : -1;
+    } else {
+      const int lat = lat0 + r;
+      return lat < nlat ? lat : -1;
+    }
+  }
+};
+
+// Shared memory of a CTA with NB row blocks (floats2):
+//   twq[TWQ] | NB x rows[R][RP]
+template <class C>
+constexpr long ts_f2_smem_bytes(int nb) {
+  return (long)sizeof(float2) * (C::TWQ + (long)nb * C::R * C::RP);
+}
+
+// ---------------------------------------------------------------- kernels
+
+// fm[field][m][lat] -> spat[field][lat][phi].  grid = (ceil(nlat/R), fields),
+// block = P*R.
+template <int P, int Q, int R>
+__global__ void __launch_bounds__(P *R)
+ts_f2_synth(TsFftTab ft, const float2 *__restrict__ fm, long fm_stride, float *__restrict__ spat,
+            long spat_stride) {
+  using C = TsF2<P, Q, R>;
+  extern __shared__ float2 ts_smem_f2s[];
+  float2 *twq = ts_smem_f2s;
+  float2 *b = twq + C::TWQ;
+  const long f = blockIdx.y;
+  const TsF2Rows<C, false> rows{(int)blockIdx.x * R, ft.nlat, 0};
+  ts_f2_twq<C>(twq, ft);
+  ts_f2_pack<C>(b, fm + f * fm_stride, ft, rows);
+  __syncthreads();
+  ts_f2_inverse<C>(b, twq);
+  ts_f2_store_rows<C>(b, spat + f * spat_stride, ft.nphi, rows);
+}
+
+// spat[field][lat][phi] -> g[field][m][lat].  grid = (ceil(nlat/R), fields).
+template <int P, int Q, int R>
+__global__ void __launch_bounds__(P *R)
+ts_f2_analys(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
+             float2 *__restrict__ g, long g_stride) {
+  using C = TsF2<P, Q, R>;
+  extern __shared__ float2 ts_smem_f2a[];
+  float2 *twq = ts_smem_f2a;
+  float2 *b = twq + C::TWQ;
+  const long f = blockIdx.y;
+  const TsF2Rows<C, false> rows{(int)blockIdx.x * R, ft.nlat, 0};
+  ts_f2_twq<C>(twq, ft);
+  ts_f2_load_rows<C>(b, spat + f * spat_stride, ft.nphi, rows);
+  __syncthreads();
+  ts_f2_forward<C>(b, twq);
+  ts_f2_unpack<C>(b, g + f * g_stride, ft, rows);
+}
+
+// spat[field][lat][phi] -> W image.  grid = (ceil(nh/(R/2)), fields).
+template <int P, int Q, int R>
+__global__ void __launch_bounds__(P *R)
+ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
+               const float *__restrict__ wq, char *wimg, int nfb, int fpb, int nlc, int nh) {
+  using C = TsF2<P, Q, R>;
+  extern __shared__ float2 ts_smem_f2w[];
+  float2 *twq = ts_smem_f2w;
+  float2 *b = twq + C::TWQ;
+  const long f = blockIdx.y;
+  const int lat0 = blockIdx.x * (R / 2);
+  const TsF2Rows<C, true> rows{lat0, ft.nlat, nh};
+  ts_f2_twq<C>(twq, ft);
+  ts_f2_load_rows<C>(b, spat + f * spat_stride, ft.nphi, rows);
+  __syncthreads();
+  ts_f2_forward<C>(b, twq);
+  ts_f2_write_w<C>(b, lat0, f, ft, wq, wimg, nfb, fpb, nlc, nh);
+}
+
+// ------------------------------------------------------- fused grid phase
+//
+// One launch runs a whole grid phase of a compiled model for R latitude rows
+// of one instance: the synthesis of the phase's NSYN spectral inputs, the
+// generated element-wise program at every grid point (Prog::eval, two points
+// per packed complex value), and the analysis of its NANA outputs.  The grid
+// values stay in shared memory; a grid variable reaches HBM only when it is
+// materialised (NGOUT outputs: a displayed field, or a value a later phase
+// reads).  PAIRED (tensor-core plans) takes latitude pairs and writes the
+// analysis as the W image, otherwise it writes
+//   gm [inst][NANA][mmax+1][nlat].
+// grid = (ceil(nlat/R) or ceil(nh/(R/2)), instances), block = P*R; shared
+// memory ts_f2_smem_bytes(max(NSYN + NGIN, NANA, 1)).
+template <class Prog, int P, int Q, int R, bool PAIRED>
+__global__ void __launch_bounds__(P *R) ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
+  using C = TsF2<P, Q, R>;
+  constexpr int NSYN = Prog::NSYN, NGIN = Prog::NGIN, NANA = Prog::NANA, NGOUT = Prog::NGOUT;
+  constexpr int NIN = NSYN + NGIN;
+  constexpr int NB = NIN > NANA ? (NIN > 0 ? NIN : 1) : (NANA > 0 ? NANA : 1);
+  extern __shared__ float2 ts_smem_f2p[];
+  float2 *twq = ts_smem_f2p;
+  float2 *buf = twq + C::TWQ;
+  constexpr int BS = C::R * C::RP;  // floats2 per row block
+  const long inst = blockIdx.y;
+  const int lat0 = blockIdx.x * (PAIRED ? R / 2 : R);
+  const TsF2Rows<C, PAIRED> rows{lat0, ft.nlat, io.nh};
+  ts_f2_twq<C>(twq, ft);
+#pragma unroll
+  for (int s = 0; s < NSYN; s++)
+    ts_f2_pack<C>(buf + s * BS, io.fm + (inst * NSYN + s) * io.field, ft, rows);
+#pragma unroll
+  for (int gi = 0; gi < NGIN; gi++)
+    ts_f2_load_rows<C>(buf + (NSYN + gi) * BS, io.gin[gi] + inst * io.gin_stride[gi], ft.nphi,
+                       rows);
+  __syncthreads();
+#pragma unroll 1
+  for (int s = 0; s < NSYN; s++) ts_f2_inverse<C>(buf + s * BS, twq);
+
+  // the element-wise program: every input of a point is read before its
+  // outputs overwrite the same position of the first NANA blocks
+  const float *prm = io.prm + inst * io.nprm;
+  for (int i = threadIdx.x; i < C::R * C::H; i += C::T) {
+    const int r = i / C::H, n = i - r * C::H;
+    const int lat = rows(r);
+    if (lat < 0) continue;
+    const int pos = r * C::RP + n;
+    float in0[NIN > 0 ? NIN : 1], in1[NIN > 0 ? NIN : 1];
+#pragma unroll
+    for (int k = 0; k < NIN; k++) {
+      const float2 z = buf[k * BS + pos];
+      in0[k] = z.x;
+      in1[k] = z.y;
+    }
+    float out0[NANA + NGOUT > 0 ? NANA + NGOUT : 1], out1[NANA + NGOUT > 0 ? NANA + NGOUT : 1];
+    Prog::eval(in0, out0, prm);
+    Prog::eval(in1, out1, prm);
+#pragma unroll
+    for (int k = 0; k < NANA; k++) buf[k * BS + pos] = make_float2(out0[k], out1[k]);
+#pragma unroll
+    for (int o = 0; o < NGOUT; o++)
+      reinterpret_cast<float2 *>(io.gout[o] + inst * io.gout_stride[o] + (long)lat * ft.nphi)[n] =
+          make_float2(out0[NANA + o], out1[NANA + o]);
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int k = 0; k < NANA; k++) ts_f2_forward<C>(buf + k * BS, twq);
+#pragma unroll
+  for (int k = 0; k < NANA; k++) {
+    if constexpr (PAIRED)
+      ts_f2_write_w<C>(buf + k * BS, lat0, inst * NANA + k, ft, io.wq, io.wimg, io.w_nfb,
+                       io.w_fpb, io.w_nlc, io.nh);
+    else
+      ts_f2_unpack<C>(buf + k * BS, io.gm + (inst * NANA + k) * io.field, ft, rows);
+  }
+}

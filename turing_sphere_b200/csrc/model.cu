@@ -56,7 +56,8 @@ struct Stage {
   cudaKernel_t kern = nullptr;
   std::vector<Ref> in, out;
   int nsyn = 0, nana = 0;
-  int lb = 0, F = 1, K = 1, W = 1, per_cta = 1, r1 = 0;
+  int lb = 0, F = 1, K = 1, W = 1, per_cta = 1;
+  int threads = 0;    // phase: threads per CTA (two-phase FFT: P*R, lb = R rows)
   bool wimg = false;  // tensor-core plan: the phase writes the W image itself
   size_t smem = 0;
   std::string label;  // one line, for describe()
@@ -412,12 +413,19 @@ void schedule(ts_model m, Program &P, bool is_step) {
       for (size_t o = 0; o < gout.size(); o++)
         src << "    out[" << A.size() + o << "] = " << em.name.at(gout[o]) << ";\n";
       src << "  }\n};\n";
-      const int r1 = ts_fft_r1(p);
-      const bool tcw = p->precision != TS_PREC_FP32 && r1 && !A.empty();
-      st.expr = tcw  ? "ts_fourier_phase_rw<" + pn + ", " + std::to_string(r1) + ">"
-                : r1 ? "ts_fourier_phase_r<" + pn + ", " + std::to_string(r1) + ">"
-                     : "ts_fourier_phase<" + pn + ">";
-      st.r1 = r1;
+      // two-phase FFT when the row length has a shape and the row blocks fit
+      int fP = 0, fQ = 0, fR = 0;
+      const int nb = std::max<int>({(int)(S.size() + gin.size()), (int)A.size(), 1});
+      if (ts_f2_shape(p, &fP, &fQ)) fR = ts_f2_phase_rows(p, nb, &st.smem);
+      const bool tcw = p->precision != TS_PREC_FP32 && fR && !A.empty();
+      if (fR) {
+        st.expr = "ts_f2_phase<" + pn + ", " + std::to_string(fP) + ", " + std::to_string(fQ) +
+                  ", " + std::to_string(fR) + ", " + (tcw ? "true" : "false") + ">";
+        st.lb = fR;
+        st.threads = fP * fR;
+      } else {
+        st.expr = "ts_fourier_phase<" + pn + ">";
+      }
       st.wimg = tcw;
       if (tcw) st.per_cta = (int)A.size() * (TS_TC_FIELDS / (int)A.size());
       st.label = "phase   " + std::to_string(S.size()) + " synth, " + std::to_string(G.size()) +
@@ -569,7 +577,7 @@ std::string stage_title(const Stage &s) { return s.label; }
 // and the lowered name of every template instantiation.
 std::vector<char> build_cubin(ts_model m, std::map<std::string, std::string> &lowered) {
   std::ostringstream src;
-  src << "#include \"ts_common.cuh\"\n#include \"fourier.cuh\"\n#include \"leg_f32.cuh\"\n"
+  src << "#include \"ts_common.cuh\"\n#include \"fft2.cuh\"\n#include \"fourier.cuh\"\n#include \"leg_f32.cuh\"\n"
       << "#include \"leg_tc.cuh\"\n";
   for (auto &P : m->prog)
     for (auto &s : P.stages) src << stage_source(s);
@@ -690,8 +698,14 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
         }
         TsFftTab ft = p->fft;
         void *args[] = {&ft, &io};
-        dim3 grid(s.wimg ? (p->nh + s.lb - 1) / s.lb : (p->nlat + s.lb - 1) / s.lb, B);
-        TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(32 * s.lb), args, s.smem, st));
+        if (s.threads) {  // two-phase FFT: R rows (R/2 latitude pairs) per CTA
+          const int per = s.wimg ? s.lb / 2 : s.lb;
+          dim3 grid(((s.wimg ? p->nh : p->nlat) + per - 1) / per, B);
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(s.threads), args, s.smem, st));
+        } else {
+          dim3 grid((p->nlat + s.lb - 1) / s.lb, B);
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(32 * s.lb), args, s.smem, st));
+        }
         break;
       }
       case Stage::LegAnalys: {
@@ -744,9 +758,7 @@ void finish_shapes(ts_model m) {
     for (auto &s : P.stages) {
       if (s.kind == Stage::Phase) {
         const int nrows = s.nsyn + s.nana + 1;
-        s.lb = s.wimg ? ts_rfft_np(p, m->batch, s.nana, &s.smem)
-               : s.r1 ? ts_rfft_lb(p, m->batch, 1, &s.smem)
-                      : ts_fourier_lb(p, m->batch, nrows, &s.smem);
+        if (!s.threads) s.lb = ts_fourier_lb(p, m->batch, nrows, &s.smem);
       } else if (s.kind == Stage::LegAnalys) {
         s.smem = p->precision != TS_PREC_FP32 ? ts_tc_analys_smem(p) : ts_analys_smem(p, s.F, s.W);
       }

@@ -103,8 +103,13 @@ size_t ts_analys_smem(ts_plan p, int F, int W);
 // rows per Fourier CTA for a kernel holding `nrows` rows per warp
 int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem);
 // warp-register FFT: R1 = H/32 (0 = not applicable) and rows per CTA
-int ts_fft_r1(ts_plan p);
-int ts_rfft_lb(ts_plan p, int nblocks_y, int nrowbuf, size_t *smem);
+// two-phase FFT (kernels/fft2.cuh): the plan's shape H = P*Q (false: none,
+// the Stockham kernels run), its shared memory, and the rows of a phase CTA
+bool ts_f2_shape(ts_plan p, int *P, int *Q);
+size_t ts_f2_bytes(int P, int Q, int R, int nb);
+int ts_f2_phase_rows(ts_plan p, int nb, size_t *smem);
+// raise a kernel's dynamic shared-memory limit on `device` (once per size)
+void ts_allow_smem(const void *fn, int device, size_t bytes);
 void ts_init_tables(ts_plan p);
 // tensor-core tables and kernels (sht_tc.cu)
 struct TsTcTab;
@@ -140,6 +145,5 @@ void ts_launch_wimage(ts_plan p, const float2 *g, long gs, int nf, int fpb, char
 bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb,
                                 char *wimg, cudaStream_t s);
 // north/south pairs per CTA of the paired Fourier kernels, and their shared memory
-int ts_rfft_np(ts_plan p, int nblocks_y, int ntiles_out, size_t *smem);
 int ts_tc_check_error(ts_plan p);
 void ts_kernel_attrs_once(ts_ctx ctx);

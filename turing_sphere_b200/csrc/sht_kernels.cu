@@ -1,8 +1,11 @@
 // Plan tables (FP64 on the GPU) and launchers of the plain FP32 transform
 // kernels.
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <type_traits>
 
+#include "kernels/fft2.cuh"
 #include "kernels/fourier.cuh"
 #include "kernels/leg_f32.cuh"
 #include "runtime.h"
@@ -369,127 +372,125 @@ void ts_launch_leg_analys(ts_plan p, const float2 *g, long gs, float2 *q, long q
   return leg_analys_f<1>(p, K, W, g, gs, q, qs, nf, s);
 }
 
-// R1 of the warp-register FFT (H = 32 R1), 0 when the row does not fit it
-int ts_fft_r1(ts_plan p) {
-  if (p->fourier != TS_FOURIER_FFT) return 0;
-  const int H = p->fft.H;
-  if (H % 32) return 0;
-  const int r1 = H / 32;
-  switch (r1) {
-    case 1: case 2: case 3: case 4: case 6: case 8: case 12: case 16: case 24: return r1;
-    default: return 0;
+// Two-phase FFT shapes: H = P*Q with P, Q in-register DFT lengths, and the
+// rows R of a transform CTA (P*R threads)
+#define TS_F2_SHAPES(X) \
+  X(32, 8, 4, 16)       \
+  X(48, 8, 6, 16)       \
+  X(64, 8, 8, 16)       \
+  X(96, 12, 8, 16)      \
+  X(128, 16, 8, 16)     \
+  X(192, 16, 12, 16)    \
+  X(256, 16, 16, 16)    \
+  X(384, 24, 16, 16)    \
+  X(512, 32, 16, 16)    \
+  X(768, 32, 24, 16)    \
+  X(1024, 32, 32, 16)   \
+  X(1536, 48, 32, 8)
+
+bool ts_f2_shape(ts_plan p, int *P, int *Q) {
+  if (p->fourier != TS_FOURIER_FFT) return false;
+  switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rr) \
+  case h:                         \
+    *P = pp;                      \
+    *Q = qq;                      \
+    return true;
+    TS_F2_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+    default:
+      return false;
   }
 }
 
-// rows per register-FFT CTA: enough CTAs to fill the GPU twice, <= 8
-int ts_rfft_lb(ts_plan p, int nblocks_y, int nrowbuf, size_t *smem) {
-  int lb = 8;
-  for (; lb > 1; lb >>= 1) {
-    const long ctas = (long)nblocks_y * ((p->nlat + lb - 1) / lb);
-    if (ctas >= 2L * p->ctx->sm_count) break;
-  }
-  *smem = sizeof(float2) * ((size_t)p->nphi + p->fft.H + (size_t)lb * (p->mmax + 2) +
-                            (size_t)lb * nrowbuf * p->fft.H);
-  TS_REQUIRE(*smem <= p->ctx->smem_optin, TS_ERR_UNSUPPORTED, "grid too large for the register FFT");
-  return lb;
+size_t ts_f2_bytes(int P, int Q, int R, int nb) {
+  const int H = P * Q, RP = (H + Q) | 1;
+  return sizeof(float2) * ((size_t)Q * (P + 1) + (size_t)nb * R * RP);
 }
 
-// pairs per paired CTA: tiles tw | twr | tin (or tN) | ntiles_out*2 x [NP][P] | rowbuf
-int ts_rfft_np(ts_plan p, int nblocks_y, int ntiles_out, size_t *smem) {
-  const int nh = p->nh, P = p->mmax + 2, H = p->fft.H;
-  int np = 8;
-  auto bytes = [&](int n) {
-    return sizeof(float2) * ((size_t)p->nphi + H + (size_t)n * P * (1 + 2 * ntiles_out) +
-                             (size_t)n * H);
-  };
-  for (; np > 1; np >>= 1) {
-    const long ctas = (long)nblocks_y * ((nh + np - 1) / np);
-    if (bytes(np) <= p->ctx->smem_optin / 2 && ctas >= 2L * p->ctx->sm_count) break;
+// rows per phase CTA with nb row blocks: 16 while two CTAs fit on an SM,
+// else the largest of 8, 4 that fits at all (0: none does)
+int ts_f2_phase_rows(ts_plan p, int nb, size_t *smem) {
+  int P, Q;
+  if (!ts_f2_shape(p, &P, &Q)) return 0;
+  const size_t cap = p->ctx->smem_optin;
+  for (int R : {16, 8, 4}) {
+    const size_t b = ts_f2_bytes(P, Q, R, nb);
+    if (P * R > 1024 || b > cap) continue;
+    if (R == 16 && 2 * (b + 1024) > cap + 1024) continue;
+    *smem = b;
+    return R;
   }
-  *smem = bytes(np);
-  TS_REQUIRE(*smem <= p->ctx->smem_optin, TS_ERR_UNSUPPORTED, "grid too large for the paired FFT");
-  return np;
+  return 0;
+}
+
+void ts_allow_smem(const void *fn, int device, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> done;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t &have = done[{device, fn}];
+  if (have >= bytes) return;
+  TS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  have = bytes;
 }
 
 namespace {
-template <int R1>
-void ranalys_w(ts_plan p, const float *spat, long ss, int nf, int fpb, char *wimg, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    TS_CUDA(cudaFuncSetAttribute(ts_fourier_analys_rw<R1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)p->ctx->smem_optin));
-    attr = true;
-  }
-  size_t smem;
-  const int np = ts_rfft_np(p, nf, 1, &smem);
+template <int P, int Q, int R>
+void f2_synth(ts_plan p, const float2 *fm, long fs, float *spat, long ss, int nf, cudaStream_t s) {
+  const size_t smem = ts_f2_bytes(P, Q, R, 1);
+  ts_allow_smem((const void *)ts_f2_synth<P, Q, R>, p->ctx->device, smem);
+  dim3 grid((p->nlat + R - 1) / R, nf);
+  ts_f2_synth<P, Q, R><<<grid, P * R, smem, s>>>(p->fft, fm, fs, spat, ss);
+  TS_CUDA(cudaGetLastError());
+}
+template <int P, int Q, int R>
+void f2_analys(ts_plan p, const float *spat, long ss, float2 *g, long gs, int nf, cudaStream_t s) {
+  const size_t smem = ts_f2_bytes(P, Q, R, 1);
+  ts_allow_smem((const void *)ts_f2_analys<P, Q, R>, p->ctx->device, smem);
+  dim3 grid((p->nlat + R - 1) / R, nf);
+  ts_f2_analys<P, Q, R><<<grid, P * R, smem, s>>>(p->fft, spat, ss, g, gs);
+  TS_CUDA(cudaGetLastError());
+}
+template <int P, int Q, int R>
+void f2_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb, char *wimg,
+                 cudaStream_t s) {
+  const size_t smem = ts_f2_bytes(P, Q, R, 1);
+  ts_allow_smem((const void *)ts_f2_analys_w<P, Q, R>, p->ctx->device, smem);
   const int nlc = (p->nh + 31) / 32;
-  dim3 grid((p->nh + np - 1) / np, nf);
-  ts_fourier_analys_rw<R1><<<grid, 32 * np, smem, s>>>(p->fft, spat, ss, p->d_wq, wimg,
-                                                       (nf + fpb - 1) / fpb, fpb, nlc, p->nh);
+  dim3 grid((p->nh + R / 2 - 1) / (R / 2), nf);
+  ts_f2_analys_w<P, Q, R><<<grid, P * R, smem, s>>>(p->fft, spat, ss, p->d_wq, wimg,
+                                                    (nf + fpb - 1) / fpb, fpb, nlc, p->nh);
   TS_CUDA(cudaGetLastError());
 }
-template <int R1>
-void rsynth(ts_plan p, const float2 *fm, long fs, float *spat, long ss, int nf, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    TS_CUDA(cudaFuncSetAttribute(ts_fourier_synth_r<R1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)p->ctx->smem_optin));
-    attr = true;
-  }
-  size_t smem;
-  const int lb = ts_rfft_lb(p, nf, 1, &smem);
-  dim3 grid((p->nlat + lb - 1) / lb, nf);
-  ts_fourier_synth_r<R1><<<grid, 32 * lb, smem, s>>>(p->fft, fm, fs, spat, ss);
-  TS_CUDA(cudaGetLastError());
-}
-template <int R1>
-void ranalys(ts_plan p, const float *spat, long ss, float2 *g, long gs, int nf, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    TS_CUDA(cudaFuncSetAttribute(ts_fourier_analys_r<R1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)p->ctx->smem_optin));
-    attr = true;
-  }
-  size_t smem;
-  const int lb = ts_rfft_lb(p, nf, 1, &smem);
-  dim3 grid((p->nlat + lb - 1) / lb, nf);
-  ts_fourier_analys_r<R1><<<grid, 32 * lb, smem, s>>>(p->fft, spat, ss, g, gs);
-  TS_CUDA(cudaGetLastError());
-}
-#define TS_R1_SWITCH(r1, F, ...)          \
-  switch (r1) {                           \
-    case 1: return F<1>(__VA_ARGS__);     \
-    case 2: return F<2>(__VA_ARGS__);     \
-    case 3: return F<3>(__VA_ARGS__);     \
-    case 4: return F<4>(__VA_ARGS__);     \
-    case 6: return F<6>(__VA_ARGS__);     \
-    case 8: return F<8>(__VA_ARGS__);     \
-    case 12: return F<12>(__VA_ARGS__);   \
-    case 16: return F<16>(__VA_ARGS__);   \
-    case 24: return F<24>(__VA_ARGS__);   \
-  }
 }  // namespace
 
 bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb,
                                 char *wimg, cudaStream_t s) {
-  switch (ts_fft_r1(p)) {
-    case 1: ranalys_w<1>(p, spat, ss, nf, fpb, wimg, s); return true;
-    case 2: ranalys_w<2>(p, spat, ss, nf, fpb, wimg, s); return true;
-    case 3: ranalys_w<3>(p, spat, ss, nf, fpb, wimg, s); return true;
-    case 4: ranalys_w<4>(p, spat, ss, nf, fpb, wimg, s); return true;
-    case 6: ranalys_w<6>(p, spat, ss, nf, fpb, wimg, s); return true;
-    case 8: ranalys_w<8>(p, spat, ss, nf, fpb, wimg, s); return true;
-    case 12: ranalys_w<12>(p, spat, ss, nf, fpb, wimg, s); return true;
-    case 16: ranalys_w<16>(p, spat, ss, nf, fpb, wimg, s); return true;
-    case 24: ranalys_w<24>(p, spat, ss, nf, fpb, wimg, s); return true;
-    default: return false;
+  if (p->fourier != TS_FOURIER_FFT) return false;
+  switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rr) \
+  case h:                         \
+    f2_analys_w<pp, qq, rr>(p, spat, ss, nf, fpb, wimg, s); \
+    return true;
+    TS_F2_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+    default:
+      return false;
   }
 }
 
 void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, long ss, int nf,
                              cudaStream_t s) {
-  if (const int r1 = ts_fft_r1(p)) {
-    TS_R1_SWITCH(r1, rsynth, p, fm, fs, spat, ss, nf, s)
+  if (p->fourier == TS_FOURIER_FFT) {
+    switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rr) \
+  case h:                         \
+    return f2_synth<pp, qq, rr>(p, fm, fs, spat, ss, nf, s);
+      TS_F2_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+      default:
+        break;
+    }
   }
   if (p->fourier == TS_FOURIER_DFT) {
     dim3 grid((p->nphi + 63) / 64, p->nlat, nf);
@@ -506,8 +507,16 @@ void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, 
 
 void ts_launch_fourier_analys(ts_plan p, const float *spat, long ss, float2 *g, long gs, int nf,
                               cudaStream_t s) {
-  if (const int r1 = ts_fft_r1(p)) {
-    TS_R1_SWITCH(r1, ranalys, p, spat, ss, g, gs, nf, s)
+  if (p->fourier == TS_FOURIER_FFT) {
+    switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rr) \
+  case h:                         \
+    return f2_analys<pp, qq, rr>(p, spat, ss, g, gs, nf, s);
+      TS_F2_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+      default:
+        break;
+    }
   }
   if (p->fourier == TS_FOURIER_DFT) {
     dim3 grid((p->mmax + 1 + 63) / 64, p->nlat, nf);

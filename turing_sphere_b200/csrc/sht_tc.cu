@@ -266,7 +266,7 @@ __global__ void ts_k_qimage(TsLegTab t, TsTcTab tc, TsFields q, int nfields, cha
 }
 
 // G[field][m][lat] -> raw fp32 W image (the fold the Fourier analysis does
-// itself when it can: see ts_fourier_analys_rw).  grid = (nLC, nfb*2, mmax+1),
+// itself when it can: see ts_f2_analys_w).  grid = (nLC, nfb*2, mmax+1),
 // block = 256: warp -> 8 fields, lane -> latitude of the chunk
 __global__ void ts_k_wimage(TsLegTab t, const float2 *g, long gs, int nfields, int fpb, int nfb,
                             int nlc, char *img) {
@@ -328,12 +328,7 @@ void ts_launch_wimage(ts_plan p, const float2 *g, long gs, int nf, int fpb, char
 
 void ts_launch_synth_tc_img(ts_plan p, const char *qimg, int nf, float2 *fm, long fs,
                             cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    TS_CUDA(cudaFuncSetAttribute(ts_leg_synth_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)p->ctx->smem_optin));
-    attr = true;
-  }
+  ts_allow_smem((const void *)ts_leg_synth_tc, p->ctx->device, ts_tc_synth_smem(p));
   const TsTcTab &tc = ts_tc_tab(p);
   const int nfb = (nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS;
   const int ctas = ts_tc_ctas(p, (long)(p->mmax + 1) * tc.nLT * nfb);
@@ -354,13 +349,8 @@ void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fs, i
 
 void ts_launch_analys_tc_img(ts_plan p, const char *wimg, int nf, float2 *out, long os,
                              cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    TS_CUDA(cudaFuncSetAttribute(ts_leg_analys_tc<TsAnalysStore>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)p->ctx->smem_optin));
-    attr = true;
-  }
+  ts_allow_smem((const void *)ts_leg_analys_tc<TsAnalysStore>, p->ctx->device,
+                ts_tc_analys_smem(p));
   const int nfb = (nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS;
   const int ntile = ts_tc_ntile(p);
   const int ctas = ts_tc_ctas(p, (long)(p->mmax + 1) * 2 * ntile * nfb);
