@@ -248,30 +248,40 @@ TS_DEV void ts_f2_forward(float2 *b, const float2 *twq) {
 
 // Z of the synthesis for the CTA's rows from the spectra src[k*nlat + lat]
 // of one field.  lat_of(r) < 0 marks a row without a latitude (zeros).
-// Thread i takes the pair (k, H-k), k = i / R, of row i % R: consecutive
-// threads read consecutive latitudes.
+// Item i is the pair (k, H-k), k = i / R, of row i % R: consecutive threads
+// read consecutive latitudes.  Every load of a thread is issued before the
+// first is used.
 template <class C, class LatOf>
 TS_DEV void ts_f2_pack(float2 *b, const float2 *__restrict__ src, const TsFftTab &ft,
                        LatOf lat_of) {
-  constexpr int H = C::H, NK = H / 2 + 1;
-  for (int i = threadIdx.x; i < NK * C::R; i += C::T) {
+  constexpr int H = C::H, NK = H / 2 + 1, NI = (NK * C::R + C::T - 1) / C::T;
+  float2 xk[NI], xh[NI];
+#pragma unroll
+  for (int j = 0; j < NI; j++) {
+    const int i = threadIdx.x + j * C::T;
     const int kk = i / C::R, r = i - kk * C::R;
-    const int h = H - kk;
-    const int lat = lat_of(r);
-    float2 xk = make_float2(0.f, 0.f), xh = make_float2(0.f, 0.f);
+    const int lat = i < NK * C::R ? lat_of(r) : -1;
+    xk[j] = make_float2(0.f, 0.f);
+    xh[j] = make_float2(0.f, 0.f);
     if (lat >= 0) {
-      if (kk <= ft.mmax) {
-        xk = src[(long)kk * ft.nlat + lat];
-        if (kk == 0) xk.y = 0.f;
-      }
-      if (h <= ft.mmax) xh = src[(long)h * ft.nlat + lat];
+      if (kk <= ft.mmax) xk[j] = src[(long)kk * ft.nlat + lat];
+      if (H - kk <= ft.mmax) xh[j] = src[(long)(H - kk) * ft.nlat + lat];
     }
-    float2 *row = b + r * C::RP;
-    const float2 ch = c_conj(xh);
-    row[kk] = c_add(c_add(xk, ch), c_mul_i(c_mul(c_sub(xk, ch), __ldg(ft.tw + kk))));
-    if (kk > 0 && kk < h) {
-      const float2 ck = c_conj(xk);
-      row[h] = c_add(c_add(xh, ck), c_mul_i(c_mul(c_sub(xh, ck), __ldg(ft.tw + h))));
+  }
+#pragma unroll
+  for (int j = 0; j < NI; j++) {
+    const int i = threadIdx.x + j * C::T;
+    if (i < NK * C::R) {
+      const int kk = i / C::R, r = i - kk * C::R;
+      const int h = H - kk;
+      float2 *row = b + r * C::RP;
+      const float2 x = kk == 0 ? make_float2(xk[j].x, 0.f) : xk[j];
+      const float2 ch = c_conj(xh[j]);
+      row[kk] = c_add(c_add(x, ch), c_mul_i(c_mul(c_sub(x, ch), __ldg(ft.tw + kk))));
+      if (kk > 0 && kk < h) {
+        const float2 ck = c_conj(x);
+        row[h] = c_add(c_add(xh[j], ck), c_mul_i(c_mul(c_sub(xh[j], ck), __ldg(ft.tw + h))));
+      }
     }
   }
 }
@@ -301,11 +311,21 @@ TS_DEV void ts_f2_unpack(const float2 *b, float2 *__restrict__ dst, const TsFftT
 // grid rows: b <-> rows of src/dst (row `lat` starts at lat*nphi floats)
 template <class C, class LatOf>
 TS_DEV void ts_f2_load_rows(float2 *b, const float *__restrict__ src, int nphi, LatOf lat_of) {
-  for (int i = threadIdx.x; i < C::R * C::H; i += C::T) {
+  constexpr int NI = (C::R * C::H + C::T - 1) / C::T;
+  float2 v[NI];
+#pragma unroll
+  for (int j = 0; j < NI; j++) {
+    const int i = threadIdx.x + j * C::T;
     const int r = i / C::H, n = i - r * C::H;
-    const int lat = lat_of(r);
-    b[r * C::RP + n] = lat >= 0 ? reinterpret_cast<const float2 *>(src + (long)lat * nphi)[n]
-                                : make_float2(0.f, 0.f);
+    const int lat = i < C::R * C::H ? lat_of(r) : -1;
+    v[j] = lat >= 0 ? reinterpret_cast<const float2 *>(src + (long)lat * nphi)[n]
+                    : make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int j = 0; j < NI; j++) {
+    const int i = threadIdx.x + j * C::T;
+    const int r = i / C::H, n = i - r * C::H;
+    if (i < C::R * C::H) b[r * C::RP + n] = v[j];
   }
 }
 
@@ -383,10 +403,16 @@ constexpr long ts_f2_smem_bytes(int nb) {
 
 // ---------------------------------------------------------------- kernels
 
+// resident CTAs per SM asked of the register allocator: three for the
+// 384-thread shapes up to P = 24 (<= 56 registers), else whatever fits
+#ifndef TS_F2_MINB
+#define TS_F2_MINB(P, R) ((P) <= 24 && (P) * (R) <= 384 ? 3 : 1)
+#endif
+
 // fm[field][m][lat] -> spat[field][lat][phi].  grid = (ceil(nlat/R), fields),
 // block = P*R.
 template <int P, int Q, int R>
-__global__ void __launch_bounds__(P *R)
+__global__ void __launch_bounds__(P *R, TS_F2_MINB(P, R))
 ts_f2_synth(TsFftTab ft, const float2 *__restrict__ fm, long fm_stride, float *__restrict__ spat,
             long spat_stride) {
   using C = TsF2<P, Q, R>;
@@ -404,7 +430,7 @@ ts_f2_synth(TsFftTab ft, const float2 *__restrict__ fm, long fm_stride, float *_
 
 // spat[field][lat][phi] -> g[field][m][lat].  grid = (ceil(nlat/R), fields).
 template <int P, int Q, int R>
-__global__ void __launch_bounds__(P *R)
+__global__ void __launch_bounds__(P *R, TS_F2_MINB(P, R))
 ts_f2_analys(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
              float2 *__restrict__ g, long g_stride) {
   using C = TsF2<P, Q, R>;
@@ -422,7 +448,7 @@ ts_f2_analys(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
 
 // spat[field][lat][phi] -> W image.  grid = (ceil(nh/(R/2)), fields).
 template <int P, int Q, int R>
-__global__ void __launch_bounds__(P *R)
+__global__ void __launch_bounds__(P *R, TS_F2_MINB(P, R))
 ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
                const float *__restrict__ wq, char *wimg, int nfb, int fpb, int nlc, int nh) {
   using C = TsF2<P, Q, R>;

@@ -206,6 +206,7 @@ struct TsTcPipe {
 #define TS_TC_SYN_ROW 68
 #define TS_TC_SYN_STAGING (TS_TC_FIELDS * TS_TC_SYN_ROW * 4)
 #define TS_TC_ANA_ROW (TS_TC_FIELDS + 1)
+#define TS_TC_ANA_COLS 64  // accumulator columns staged at a time by the analysis
 
 // barrier of the 4 epilogue warps (named barrier 1).  Every epilogue warp
 // runs the same sequence of these (exits are decided uniformly, through
@@ -601,7 +602,8 @@ struct TsAnalysSched {
 
 // grid = min(#SMs, tiles), block = 320, persistent.  Tiles with no l values
 // have no stages; their epilogue does nothing.  Dynamic shared memory:
-// S*(2*16384 + 2*Nmax*128) + Nmax*2*TS_TC_ANA_ROW*4 + 1024 + sizeof(TsTcPipe).  TMEM:
+// S*(2*16384 + 2*Nmax*128) + min(Nmax, TS_TC_ANA_COLS)*2*TS_TC_ANA_ROW*4 + 1024
+// + sizeof(TsTcPipe).  TMEM:
 // two buffers of 256 columns.
 template <class Epi>
 __global__ void __launch_bounds__(TS_TC_THREADS, 1)
@@ -612,7 +614,8 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned stage = 2 * 16384 + 2 * nmax * 128;
   float *sD = reinterpret_cast<float *>(smem + S * stage);
-  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + nmax * 2 * TS_TC_ANA_ROW * 4);
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage +
+                                               min(nmax, TS_TC_ANA_COLS) * 2 * TS_TC_ANA_ROW * 4);
   const TsAnalysSched sc{&tc, t.lmax, t.mmax, w_nfb, ntile, wimg};
   ts_tc_pipe_init(pp, S);
   if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
@@ -630,21 +633,25 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
     const int N = ts_round16(cnt);
     const int row = ts_epi_row(warp, lane), fl = row >> 1, comp = row & 1;
     const unsigned lanebase = tbase + ((unsigned)((warp & 3) * 32) << 16);
-    ts_epi_bar();  // the previous tile's epi calls are done with sD
-    for (int c0 = 0; c0 < N; c0 += 16) {
-      float v[16];
-      ts_tmem_ld16(lanebase + (unsigned)c0, v);
-#pragma unroll
-      for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_ANA_ROW + fl] = v[i];
-    }
-    ts_epi_bar();
     const int f0 = fb * per_cta;
     const int nf = min(per_cta, nfields - f0);
     const long base = ts_lm_base(t.lmax, m);
-    for (int idx = (warp & 3) * 32 + lane; idx < cnt * 2; idx += 128) {
-      const int j = idx >> 1, cp = idx & 1;
-      const int l = m + par + 2 * (lt * tc.LTL + j);
-      epi(base + (l - m), cp, sD + (j * 2 + cp) * TS_TC_ANA_ROW, f0, nf, TS_TC_FIELDS);
+    for (int h0 = 0; h0 < N; h0 += TS_TC_ANA_COLS) {
+      const int hn = min(TS_TC_ANA_COLS, N - h0);
+      ts_epi_bar();  // the previous epi calls are done with sD
+      for (int c0 = 0; c0 < hn; c0 += 16) {
+        float v[16];
+        ts_tmem_ld16(lanebase + (unsigned)(h0 + c0), v);
+#pragma unroll
+        for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_ANA_ROW + fl] = v[i];
+      }
+      ts_epi_bar();
+      const int jn = min(hn, cnt - h0);
+      for (int idx = (warp & 3) * 32 + lane; idx < jn * 2; idx += 128) {
+        const int jj = idx >> 1, cp = idx & 1;
+        const int l = m + par + 2 * (lt * tc.LTL + h0 + jj);
+        epi(base + (l - m), cp, sD + (jj * 2 + cp) * TS_TC_ANA_ROW, f0, nf, TS_TC_FIELDS);
+      }
     }
   };
   ts_tc_persistent(smem, pp, S, stage, tmem, 256, sc, epilogue);

@@ -213,7 +213,9 @@ void schedule(ts_model m, Program &P, bool is_step) {
     P.swaps.insert(st);
   }
   // lazily evaluated views: v = synth(S) of a state input S that this
-  // program advances, read nowhere else
+  // program advances.  The step may use v itself (a reaction term); the
+  // displayed field is only computed when it is read, from the state the
+  // last step started from (the second buffer of S's pair)
   std::set<int> lazy;
   if (is_step) {
     for (size_t o = m->state.size(); o < f.output_vars.size(); o++) {
@@ -222,9 +224,7 @@ void schedule(ts_model m, Program &P, bool is_step) {
         if (s.kind == tsm::Stmt::Synth && s.out == v && f.vars[s.arg].param_index >= 0) {
           const std::string &src = f.vars[s.arg].name;
           bool is_state = std::find(m->state.begin(), m->state.end(), src) != m->state.end();
-          int other_users = 0;
-          for (int u : users[v]) (void)u, other_users++;
-          if (is_state && other_users == 0) {
+          if (is_state) {
             lazy.insert(v);
             P.lazy_views[f.output_names[o]] = src;
           }
@@ -443,7 +443,12 @@ void schedule(ts_model m, Program &P, bool is_step) {
     for (int i : A) aouts.insert(f.body[i].out);
     std::vector<int> E;
     std::set<int> elocal = aouts;
-    for (size_t i = 0; i < f.body.size(); i++) {
+    // On tensor-core plans each epilogue thread walks every instance of its
+    // 64-field block for one coefficient; with many instances that loop of
+    // dependent state loads is latency-bound, so the analysis only stores and
+    // the spectral statements run as a coalesced element-wise stage (A).
+    const bool fuse_epi = p->precision == TS_PREC_FP32 || m->batch * (long)A.size() <= 16;
+    for (size_t i = 0; i < f.body.size() && fuse_epi; i++) {
       const auto &s = f.body[i];
       if (done[i] || s.kind != tsm::Stmt::Elementwise || f.vars[s.out].dom != Dom::Spec) continue;
       bool ok = true, uses_a = false;

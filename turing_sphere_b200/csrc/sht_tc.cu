@@ -219,7 +219,9 @@ int synth_stages(ts_plan p) {
 }
 int analys_N(ts_plan p) { return std::min(ts_tc_geom(p).LTL, ((kpar_h(p->lmax, 0, 0) + 15) / 16) * 16); }
 size_t analys_stage(ts_plan p) { return 2 * 16384 + 2 * (size_t)analys_N(p) * 128; }
-size_t analys_staging(ts_plan p) { return (size_t)analys_N(p) * 2 * TS_TC_ANA_ROW * 4; }
+size_t analys_staging(ts_plan p) {
+  return (size_t)std::min(analys_N(p), TS_TC_ANA_COLS) * 2 * TS_TC_ANA_ROW * 4;
+}
 }  // namespace
 
 int ts_tc_synth_stages(ts_plan p) { return synth_stages(p); }
