@@ -152,6 +152,19 @@ int ts_sht_fourier_analys_dev(ts_plan plan, const float *spat, float *fm, int ba
                               void *stream);
 int ts_sht_leg_analys_dev(ts_plan plan, const float *fm, float *qlm, int batch, void *stream);
 
+/* The two stages of ts_sht_analys_dev on a tensor-core plan, for timing them
+ * apart (no reference counterpart: the reference has one analysis path).  The
+ * Fourier analysis writes the folded, weighted operand image of the
+ * tensor-core Legendre analysis (ts_sht_wimage_bytes(plan, batch) bytes; the
+ * caller zero-fills it once, the stage writes every entry that is not
+ * padding); the Legendre stage reads it.  TS_ERR_UNSUPPORTED on an FP32 plan
+ * or a row length without a two-phase FFT shape. */
+size_t ts_sht_wimage_bytes(ts_plan plan, int batch);
+int ts_sht_fourier_analys_w_dev(ts_plan plan, const float *spat, void *wimage, int batch,
+                                void *stream);
+int ts_sht_leg_analys_w_dev(ts_plan plan, const void *wimage, float *qlm, int batch,
+                            void *stream);
+
 /* --------------------------------------------------------------- models
  * A .m model (init/step functions, src/mgpu/model.ts:1-19) compiled for a
  * plan's grid: parsed and specialised (src/mgpu/compile.ts:83-190), every

@@ -77,3 +77,28 @@ def test_tc_and_plain_both_within_tolerance(device, lmax, nlat, nphi):
     fa, fb = O.rel_l2(a.analys(s32), q64), O.rel_l2(b.analys(s32), q64)
     print(f"analys relL2 vs f64: fp32 {fa:.2e}, tf32x3 {fb:.2e}")
     assert fa < TOL and fb < TOL
+
+
+def test_w_stages_equal_analys_dev(device):
+    """fourAnalysW then legAnalysW run exactly the kernels of analys_dev on a
+    tensor-core plan, so the coefficients agree bit for bit; both stages are
+    refused on an FP32 plan."""
+    import torch
+    lmax, nlat, nphi, B = 63, 96, 192, 70
+    plan = tc_plan(device, lmax, nlat, nphi)
+    rng = np.random.default_rng(5)
+    spat = torch.from_numpy(rng.standard_normal((B, nlat * nphi)).astype(np.float32)).cuda()
+    q1 = torch.empty(B, 2 * plan.nlm, device="cuda")
+    q2 = torch.empty_like(q1)
+    img = torch.zeros(plan.wimageBytes(B) // 4 + 1, device="cuda")
+    plan.analys_dev(spat.data_ptr(), q1.data_ptr(), B)
+    plan.stage_dev("fourAnalysW", spat.data_ptr(), img.data_ptr(), B)
+    plan.stage_dev("legAnalysW", img.data_ptr(), q2.data_ptr(), B)
+    torch.cuda.synchronize()
+    plan.status()
+    assert torch.equal(q1, q2)
+    plain = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi), {"precision": "fp32"})
+    assert plain.wimageBytes(B) == 0
+    from turing_sphere_b200._lib import TsError
+    with pytest.raises(TsError):
+        plain.stage_dev("fourAnalysW", spat.data_ptr(), img.data_ptr(), B)

@@ -91,6 +91,9 @@ SIGNATURES = {
     "ts_sht_fourier_synth_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_fourier_analys_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_leg_analys_dev": (i32, [vp, vp, vp, i32, vp]),
+    "ts_sht_wimage_bytes": (C.c_size_t, [vp, i32]),
+    "ts_sht_fourier_analys_w_dev": (i32, [vp, vp, vp, i32, vp]),
+    "ts_sht_leg_analys_w_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_model_compile": (i32, [vp, cstr, C.POINTER(cstr), i32, C.POINTER(cstr), i32,
                                C.POINTER(cstr), i32, i32, C.POINTER(vp), C.POINTER(CompileError)]),
     "ts_model_destroy": (i32, [vp]),

@@ -420,6 +420,35 @@ int ts_sht_leg_analys_dev(ts_plan p, const float *fm, float *qlm, int batch, voi
   TS_API_END(ctx)
 }
 
+size_t ts_sht_wimage_bytes(ts_plan p, int batch) {
+  if (!p || p->precision == TS_PREC_FP32 || batch < 1) return 0;
+  return ts_tc_wimg_bytes(p, batch, TS_TC_FIELDS);
+}
+
+int ts_sht_fourier_analys_w_dev(ts_plan p, const float *spat, void *wimage, int batch,
+                                void *stream) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, spat, wimage, batch);
+  TS_REQUIRE(p->precision != TS_PREC_FP32, TS_ERR_UNSUPPORTED, "FP32 plans have no W image");
+  TS_CUDA(cudaSetDevice(ctx->device));
+  TS_REQUIRE(ts_launch_fourier_analys_w(p, spat, npts_of(p), batch, TS_TC_FIELDS, (char *)wimage,
+                                        ts_pick_stream(ctx, stream)),
+             TS_ERR_UNSUPPORTED, "the plan's row length has no two-phase FFT shape");
+  TS_API_END(ctx)
+}
+
+int ts_sht_leg_analys_w_dev(ts_plan p, const void *wimage, float *qlm, int batch, void *stream) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_batch(p, wimage, qlm, batch);
+  TS_REQUIRE(p->precision != TS_PREC_FP32, TS_ERR_UNSUPPORTED, "FP32 plans have no W image");
+  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_launch_analys_tc_img(p, (const char *)wimage, batch, (float2 *)qlm, p->nlm,
+                          ts_pick_stream(ctx, stream));
+  TS_API_END(ctx)
+}
+
 }  // extern "C"
 
 // ----------------------------------------------------------------- seeding

@@ -181,7 +181,7 @@ TS_DEV long ts_atile_offset(const TsTcTab &tc, int lmax, int m, int par, int lti
   return off;
 }
 
-#define TS_TC_THREADS 320
+#define TS_TC_THREADS 448  // 14 warps: split 0-3, copy 4, MMA 5, epilogue 6-13
 #define TS_TC_MAXSTAGE 4
 
 // Persistent pipeline state.  Operand ring: full[s] the copies of slot s
@@ -204,16 +204,27 @@ struct TsTcPipe {
 // 16-byte aligned); the analysis keeps [l][re|im] rows of 64 fields padded to
 // 65 floats, so that lanes reading different rows hit different banks
 #define TS_TC_SYN_ROW 68
-#define TS_TC_SYN_STAGING (TS_TC_FIELDS * TS_TC_SYN_ROW * 4)
+#define TS_TC_SYN_STAGING (TS_TC_FIELDS * TS_TC_SYN_ROW * 4)  // per epilogue group
 #define TS_TC_ANA_ROW (TS_TC_FIELDS + 1)
-#define TS_TC_ANA_COLS 64  // accumulator columns staged at a time by the analysis
+#define TS_TC_ANA_COLS 32  // accumulator columns an analysis group stages at a time
 
-// barrier of the 4 epilogue warps (named barrier 1).  Every epilogue warp
-// runs the same sequence of these (exits are decided uniformly, through
-// TsTcPipe::epi_go), so none is left waiting.
-TS_DEV void ts_epi_bar() {
+// The epilogue runs in two groups of 4 warps (warps 6-9 and 10-13; each
+// group covers all 128 TMEM lanes) that take alternate column chunks of a
+// tile.  ts_epi_bar(g) is group g's barrier (named barrier 1 + g),
+// ts_epi_bar_all() the barrier of all 8 epilogue warps (named barrier 3).
+// Every epilogue warp runs the same sequence of these (exits are decided
+// uniformly, through TsTcPipe::epi_go), so none is left waiting.
+TS_DEV int ts_epi_group(int warp) { return (warp - 6) >> 2; }
+TS_DEV void ts_epi_bar(int g) {
   __syncwarp();
-  asm volatile("bar.sync 1, 128;" ::: "memory");
+  if (g == 0)
+    asm volatile("bar.sync 1, 128;" ::: "memory");
+  else
+    asm volatile("bar.sync 2, 128;" ::: "memory");
+}
+TS_DEV void ts_epi_bar_all() {
+  __syncwarp();
+  asm volatile("bar.sync 3, 256;" ::: "memory");
 }
 
 TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S) {
@@ -225,7 +236,7 @@ TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S) {
     }
     for (int b = 0; b < 2; b++) {
       ts_mbar_init(&pp->acc_full[b], 1);
-      ts_mbar_init(&pp->acc_empty[b], 4);
+      ts_mbar_init(&pp->acc_empty[b], 8);
     }
     ts_mbar_init(&pp->epi, 4);
     ts_mbar_init(&pp->drain, 1);
@@ -399,7 +410,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
         if (!ok) ts_tc_flag(pp);
         pp->epi_go[b] = ok && !ts_tc_bad(pp);
       }
-      ts_epi_bar();
+      ts_epi_bar_all();
       if (!*reinterpret_cast<volatile int *>(&pp->epi_go[b])) return;
       ts_tc_fence_after();
       epilogue(tile, tmem + (unsigned)(b * acc_cols));
@@ -479,7 +490,7 @@ struct TsSynthSched {
 };
 
 // grid = min(#SMs, tiles), block = 320, persistent.  Dynamic shared memory:
-// S*(2*16384 + 2*NL*128) + TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe).
+// S*(2*16384 + 2*NL*128) + 2*TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe).
 // TMEM: two buffers of 2*NL columns.
 __global__ void __launch_bounds__(TS_TC_THREADS, 1)
 ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb,
@@ -489,7 +500,7 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
   const int NL = tc.NL;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned stage = 2 * 16384 + 2 * NL * 128;
-  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + TS_TC_SYN_STAGING);
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + 2 * TS_TC_SYN_STAGING);
   const TsSynthSched sc{&tc, t.lmax, t.mmax, q_nfb, NL, tc.nLT, qimg};
   ts_tc_pipe_init(pp, S);
   if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
@@ -502,7 +513,8 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
   // and south = E-O of its component into the staging rows; then the 128
   // threads write 16-byte runs of whole complex values, north in latitude
   // order and south mirrored, 8 lanes covering one field's 128-byte run
-  float *sE = reinterpret_cast<float *>(smem + S * stage);
+  const int grp = ts_epi_group(warp);
+  float *sE = reinterpret_cast<float *>(smem + S * stage + (grp > 0 ? TS_TC_SYN_STAGING : 0));
   const bool vec = (t.nlat % 2 == 0) && (fm_stride % 2 == 0) &&
                    ((reinterpret_cast<unsigned long long>(fm) & 15) == 0);
   auto epilogue = [&](int tile, unsigned tbase) {
@@ -512,7 +524,7 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
     const int et = ts_epi_row(warp, lane);  // 0..127 = TMEM lane = 2*field + comp
     float *mine = sE + (et >> 1) * TS_TC_SYN_ROW + (et & 1);
     const unsigned lanebase = tbase + ((unsigned)((warp & 3) * 32) << 16);
-    for (int c0 = 0; c0 < NL; c0 += 16) {
+    for (int c0 = 16 * grp; c0 < NL; c0 += 32) {
       float e[16], o[16];
       ts_tmem_ld16(lanebase + (unsigned)c0, e);
       if (n1 > 0)
@@ -525,7 +537,7 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
         mine[2 * i] = e[i] + o[i];
         mine[32 + 2 * i] = e[i] - o[i];
       }
-      ts_epi_bar();
+      ts_epi_bar(grp);
 #pragma unroll 2
       for (int k = 0; k < 8; k++) {
         const int q = et + 128 * k, seg = q >> 3, part = q & 7;
@@ -554,7 +566,7 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
           }
         }
       }
-      ts_epi_bar();
+      ts_epi_bar(grp);
     }
   };
   ts_tc_persistent(smem, pp, S, stage, tmem, 2 * NL, sc, epilogue);
@@ -602,7 +614,7 @@ struct TsAnalysSched {
 
 // grid = min(#SMs, tiles), block = 320, persistent.  Tiles with no l values
 // have no stages; their epilogue does nothing.  Dynamic shared memory:
-// S*(2*16384 + 2*Nmax*128) + min(Nmax, TS_TC_ANA_COLS)*2*TS_TC_ANA_ROW*4 + 1024
+// S*(2*16384 + 2*Nmax*128) + 2*min(Nmax, TS_TC_ANA_COLS)*2*TS_TC_ANA_ROW*4 + 1024
 // + sizeof(TsTcPipe).  TMEM:
 // two buffers of 256 columns.
 template <class Epi>
@@ -613,9 +625,10 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
   char *smem = (char *)(((unsigned long long)ts_smem_at + 1023) & ~1023ull);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned stage = 2 * 16384 + 2 * nmax * 128;
-  float *sD = reinterpret_cast<float *>(smem + S * stage);
-  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage +
-                                               min(nmax, TS_TC_ANA_COLS) * 2 * TS_TC_ANA_ROW * 4);
+  const int grp = ts_epi_group(warp);
+  const int ana_stg = min(nmax, TS_TC_ANA_COLS) * 2 * TS_TC_ANA_ROW * 4;  // bytes per group
+  float *sD = reinterpret_cast<float *>(smem + S * stage + (grp > 0 ? ana_stg : 0));
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + 2 * ana_stg);
   const TsAnalysSched sc{&tc, t.lmax, t.mmax, w_nfb, ntile, wimg};
   ts_tc_pipe_init(pp, S);
   if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
@@ -636,16 +649,16 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
     const int f0 = fb * per_cta;
     const int nf = min(per_cta, nfields - f0);
     const long base = ts_lm_base(t.lmax, m);
-    for (int h0 = 0; h0 < N; h0 += TS_TC_ANA_COLS) {
+    for (int h0 = TS_TC_ANA_COLS * grp; h0 < N; h0 += 2 * TS_TC_ANA_COLS) {
       const int hn = min(TS_TC_ANA_COLS, N - h0);
-      ts_epi_bar();  // the previous epi calls are done with sD
+      ts_epi_bar(grp);  // the previous epi calls are done with sD
       for (int c0 = 0; c0 < hn; c0 += 16) {
         float v[16];
         ts_tmem_ld16(lanebase + (unsigned)(h0 + c0), v);
 #pragma unroll
         for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_ANA_ROW + fl] = v[i];
       }
-      ts_epi_bar();
+      ts_epi_bar(grp);
       const int jn = min(hn, cnt - h0);
       for (int idx = (warp & 3) * 32 + lane; idx < jn * 2; idx += 128) {
         const int jj = idx >> 1, cp = idx & 1;

@@ -733,7 +733,7 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
           const char *wimg = (const char *)m->wimg.p;
           void *args[] = {&leg, &tc, &wimg, &w_nfb, &epi, &nfields, &per_cta, &S, &nmax, &ntile};
           const int ctas = ts_tc_ctas(p, (long)(p->mmax + 1) * 2 * ntile * w_nfb);
-          TS_CUDA(cudaLaunchKernel((const void *)s.kern, dim3(ctas), dim3(320), args, s.smem, st));
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern, dim3(ctas), dim3(TS_TC_THREADS), args, s.smem, st));
         } else {
           void *args[] = {&leg, &g, &gs, &epi, &nfields, &per_cta};
           dim3 grid(p->mmax + 1, (nfields + per_cta - 1) / per_cta);

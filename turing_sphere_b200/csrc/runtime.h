@@ -135,6 +135,14 @@ void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fm_st
 void ts_launch_leg_analys_tc(ts_plan p, const float2 *g, long g_stride, float2 *q, long q_stride,
                              int nfields, cudaStream_t s);
 // TC analysis from the grid: spat -> w image -> q
+#ifndef TS_TC_FIELDS
+#define TS_TC_FIELDS 64  // fields per tensor-core block (kernels/leg_tc.cuh)
+#endif
+#ifndef TS_TC_THREADS
+#define TS_TC_THREADS 448  // threads of a tensor-core Legendre CTA (kernels/leg_tc.cuh)
+#endif
+void ts_launch_analys_tc_img(ts_plan p, const char *wimg, int nf, float2 *out, long os,
+                             cudaStream_t s);
 void ts_analys_tc_full(ts_plan p, const float *spat, long spat_stride, float *qlm, int nfields,
                        cudaStream_t s);
 size_t ts_tc_qimg_bytes(ts_plan p, int nfields);

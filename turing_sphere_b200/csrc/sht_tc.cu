@@ -215,12 +215,12 @@ namespace {
 const size_t kSmemBudget = 227 * 1024 - 2048;
 size_t synth_stage(ts_plan p) { return 2 * 16384 + 2 * (size_t)ts_tc_geom(p).NL * 128; }
 int synth_stages(ts_plan p) {
-  return (int)std::min<size_t>(TS_TC_MAXSTAGE, (kSmemBudget - TS_TC_SYN_STAGING) / synth_stage(p));
+  return (int)std::min<size_t>(TS_TC_MAXSTAGE, (kSmemBudget - 2 * TS_TC_SYN_STAGING) / synth_stage(p));
 }
 int analys_N(ts_plan p) { return std::min(ts_tc_geom(p).LTL, ((kpar_h(p->lmax, 0, 0) + 15) / 16) * 16); }
 size_t analys_stage(ts_plan p) { return 2 * 16384 + 2 * (size_t)analys_N(p) * 128; }
 size_t analys_staging(ts_plan p) {
-  return (size_t)std::min(analys_N(p), TS_TC_ANA_COLS) * 2 * TS_TC_ANA_ROW * 4;
+  return 2 * (size_t)std::min(analys_N(p), TS_TC_ANA_COLS) * 2 * TS_TC_ANA_ROW * 4;
 }
 }  // namespace
 
@@ -231,7 +231,7 @@ int ts_tc_analys_stages(ts_plan p) {
 int ts_tc_analys_nmax(ts_plan p) { return analys_N(p); }
 
 size_t ts_tc_synth_smem(ts_plan p) {
-  return synth_stages(p) * synth_stage(p) + TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe);
+  return synth_stages(p) * synth_stage(p) + 2 * TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe);
 }
 
 size_t ts_tc_analys_smem(ts_plan p) {

@@ -138,12 +138,21 @@ class ShtPlan:
         _lib.check(_lib.lib().ts_sht_analys_dev(self.handle, spat_ptr, qlm_ptr, batch, stream),
                    self.device.handle)
 
+    def wimageBytes(self, batch: int) -> int:
+        """Bytes of the tensor-core analysis operand image for `batch` fields
+        (0 on an FP32 plan)."""
+        return int(_lib.lib().ts_sht_wimage_bytes(self.handle, batch))
+
     def stage_dev(self, stage: str, src_ptr: int, dst_ptr: int, batch: int = 1,
                   stream: int | None = None):
         """One stage alone (encodeStage, sht.ts:362-401): legSynth | fourSynth |
-        fourAnalys | legAnalys."""
+        fourAnalys | legAnalys, and on tensor-core plans the two stages of
+        analys_dev: fourAnalysW (grid -> operand image) | legAnalysW (image ->
+        coefficients)."""
         fn = {"legSynth": "ts_sht_leg_synth_dev", "fourSynth": "ts_sht_fourier_synth_dev",
-              "fourAnalys": "ts_sht_fourier_analys_dev", "legAnalys": "ts_sht_leg_analys_dev"}[stage]
+              "fourAnalys": "ts_sht_fourier_analys_dev", "legAnalys": "ts_sht_leg_analys_dev",
+              "fourAnalysW": "ts_sht_fourier_analys_w_dev",
+              "legAnalysW": "ts_sht_leg_analys_w_dev"}[stage]
         _lib.check(getattr(_lib.lib(), fn)(self.handle, src_ptr, dst_ptr, batch, stream),
                    self.device.handle)
 
