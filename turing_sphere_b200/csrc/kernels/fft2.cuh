@@ -254,27 +254,28 @@ TS_DEV void ts_f2_forward(float2 *b, const float2 *twq) {
 template <class C, class LatOf>
 TS_DEV void ts_f2_pack(float2 *b, const float2 *__restrict__ src, const TsFftTab &ft,
                        LatOf lat_of) {
-  constexpr int H = C::H, NK = H / 2 + 1, NI = (NK * C::R + C::T - 1) / C::T;
+  // thread t keeps row t % R and takes the pairs k = t / R + P j (T = P R)
+  constexpr int H = C::H, NK = H / 2 + 1, NI = (NK + C::P - 1) / C::P;
+  const int r = threadIdx.x % C::R, k0 = threadIdx.x / C::R;
+  const int lat = lat_of(r);
+  const float2 *col = src + (lat >= 0 ? lat : 0);
   float2 xk[NI], xh[NI];
 #pragma unroll
   for (int j = 0; j < NI; j++) {
-    const int i = threadIdx.x + j * C::T;
-    const int kk = i / C::R, r = i - kk * C::R;
-    const int lat = i < NK * C::R ? lat_of(r) : -1;
+    const int kk = k0 + C::P * j;
     xk[j] = make_float2(0.f, 0.f);
     xh[j] = make_float2(0.f, 0.f);
-    if (lat >= 0) {
-      if (kk <= ft.mmax) xk[j] = src[(long)kk * ft.nlat + lat];
-      if (H - kk <= ft.mmax) xh[j] = src[(long)(H - kk) * ft.nlat + lat];
+    if (lat >= 0 && kk < NK) {
+      if (kk <= ft.mmax) xk[j] = col[(long)kk * ft.nlat];
+      if (H - kk <= ft.mmax) xh[j] = col[(long)(H - kk) * ft.nlat];
     }
   }
+  float2 *row = b + r * C::RP;
 #pragma unroll
   for (int j = 0; j < NI; j++) {
-    const int i = threadIdx.x + j * C::T;
-    if (i < NK * C::R) {
-      const int kk = i / C::R, r = i - kk * C::R;
+    const int kk = k0 + C::P * j;
+    if (kk < NK) {
       const int h = H - kk;
-      float2 *row = b + r * C::RP;
       const float2 x = kk == 0 ? make_float2(xk[j].x, 0.f) : xk[j];
       const float2 ch = c_conj(xh[j]);
       row[kk] = c_add(c_add(x, ch), c_mul_i(c_mul(c_sub(x, ch), __ldg(ft.tw + kk))));
@@ -300,42 +301,53 @@ TS_DEV float2 ts_f2_xk(const float2 *row, int k, const TsFftTab &ft) {
 template <class C, class LatOf>
 TS_DEV void ts_f2_unpack(const float2 *b, float2 *__restrict__ dst, const TsFftTab &ft,
                          LatOf lat_of) {
-  const int n = (ft.mmax + 1) * C::R;
-  for (int i = threadIdx.x; i < n; i += C::T) {
-    const int k = i / C::R, r = i - k * C::R;
-    const int lat = lat_of(r);
-    if (lat >= 0) dst[(long)k * ft.nlat + lat] = ts_f2_xk<C>(b + r * C::RP, k, ft);
+  // thread t keeps row t % R and takes k = t / R + P j
+  const int r = threadIdx.x % C::R;
+  const int lat = lat_of(r);
+  if (lat < 0) return;
+  const float2 *row = b + r * C::RP;
+  float2 *col = dst + lat;
+  for (int k = threadIdx.x / C::R; k <= ft.mmax; k += C::P)
+    col[(long)k * ft.nlat] = ts_f2_xk<C>(row, k, ft);
+}
+
+// grid rows: b <-> rows of src/dst (row `lat` starts at lat*nphi floats).
+// Element i = (row i / H, column i % H), i = t + T j: when T is a multiple
+// of H a thread keeps one column and steps through rows.
+template <class C, class F>
+TS_DEV void ts_f2_for_rows(F &&f) {
+  constexpr int NI = (C::R * C::H + C::T - 1) / C::T;
+  if constexpr (C::T % C::H == 0) {
+    const int n = threadIdx.x % C::H, r0 = threadIdx.x / C::H;
+#pragma unroll
+    for (int j = 0; j < NI; j++) f(j, r0 + (C::T / C::H) * j, n);
+  } else {
+#pragma unroll
+    for (int j = 0; j < NI; j++) {
+      const int i = threadIdx.x + j * C::T;
+      if (i < C::R * C::H) f(j, i / C::H, i % C::H);
+    }
   }
 }
 
-// grid rows: b <-> rows of src/dst (row `lat` starts at lat*nphi floats)
 template <class C, class LatOf>
 TS_DEV void ts_f2_load_rows(float2 *b, const float *__restrict__ src, int nphi, LatOf lat_of) {
   constexpr int NI = (C::R * C::H + C::T - 1) / C::T;
   float2 v[NI];
-#pragma unroll
-  for (int j = 0; j < NI; j++) {
-    const int i = threadIdx.x + j * C::T;
-    const int r = i / C::H, n = i - r * C::H;
-    const int lat = i < C::R * C::H ? lat_of(r) : -1;
+  ts_f2_for_rows<C>([&](int j, int r, int n) {
+    const int lat = lat_of(r);
     v[j] = lat >= 0 ? reinterpret_cast<const float2 *>(src + (long)lat * nphi)[n]
                     : make_float2(0.f, 0.f);
-  }
-#pragma unroll
-  for (int j = 0; j < NI; j++) {
-    const int i = threadIdx.x + j * C::T;
-    const int r = i / C::H, n = i - r * C::H;
-    if (i < C::R * C::H) b[r * C::RP + n] = v[j];
-  }
+  });
+  ts_f2_for_rows<C>([&](int j, int r, int n) { b[r * C::RP + n] = v[j]; });
 }
 
 template <class C, class LatOf>
 TS_DEV void ts_f2_store_rows(const float2 *b, float *__restrict__ dst, int nphi, LatOf lat_of) {
-  for (int i = threadIdx.x; i < C::R * C::H; i += C::T) {
-    const int r = i / C::H, n = i - r * C::H;
+  ts_f2_for_rows<C>([&](int, int r, int n) {
     const int lat = lat_of(r);
     if (lat >= 0) reinterpret_cast<float2 *>(dst + (long)lat * nphi)[n] = b[r * C::RP + n];
-  }
+  });
 }
 
 // ------------------------------------------------- W image of the TC path
@@ -353,24 +365,26 @@ TS_DEV void ts_f2_write_w(const float2 *b, int lat0, long f, const TsFftTab &ft,
   constexpr int NPR = C::R / 2;
   const long fb = f / fpb;
   const int fl = (int)(f - fb * fpb);
-  const int n = (ft.mmax + 1) * NPR;
-  for (int i = threadIdx.x; i < n; i += C::T) {
-    const int k = i / NPR, j = i - k * NPR;
-    const int lat = lat0 + j;
-    if (lat >= nh) continue;
-    const float2 xn = ts_f2_xk<C>(b + j * C::RP, k, ft);
-    const float2 xs = (ft.nlat - 1 - lat != lat) ? ts_f2_xk<C>(b + (NPR + j) * C::RP, k, ft)
-                                                 : make_float2(0.f, 0.f);
-    const float w = __ldg(wq + lat);
-#pragma unroll
-    for (int par = 0; par < 2; par++) {
-      const long blk = (((long)k * nfb + fb) * 2 + par) * nlc + (lat >> 5);
-      char *base = wimg + blk * 16384;
-      const float re = w * (par ? xn.x - xs.x : xn.x + xs.x);
-      const float im = w * (par ? xn.y - xs.y : xn.y + xs.y);
-      *reinterpret_cast<float *>(base + ts_swz_img(2 * fl, lat & 31)) = re;
-      *reinterpret_cast<float *>(base + ts_swz_img(2 * fl + 1, lat & 31)) = im;
-    }
+  // thread t keeps latitude pair t % NPR and takes m = t / NPR + 2P j
+  const int j = threadIdx.x % NPR;
+  const int lat = lat0 + j;
+  if (lat >= nh) return;
+  const float2 *rn = b + j * C::RP, *rs = b + (NPR + j) * C::RP;
+  const bool south = ft.nlat - 1 - lat != lat;
+  const float w = __ldg(wq + lat);
+  // byte offsets of (row 2 fl + re|im, column lat % 32) inside a 16 KB block,
+  // and of this field block's chunk: block (((k nfb + fb) 2 + par) nlc + lat / 32)
+  const int o_re = ts_swz_img(2 * fl, lat & 31), o_im = ts_swz_img(2 * fl + 1, lat & 31);
+  char *base = wimg + ((long)fb * 2 * nlc + (lat >> 5)) * 16384;
+  const long kstep = (long)nfb * 2 * nlc * 16384, pstep = (long)nlc * 16384;
+  for (int k = threadIdx.x / NPR; k <= ft.mmax; k += 2 * C::P) {
+    const float2 xn = ts_f2_xk<C>(rn, k, ft);
+    const float2 xs = south ? ts_f2_xk<C>(rs, k, ft) : make_float2(0.f, 0.f);
+    char *blk = base + k * kstep;
+    *reinterpret_cast<float *>(blk + o_re) = w * (xn.x + xs.x);
+    *reinterpret_cast<float *>(blk + o_im) = w * (xn.y + xs.y);
+    *reinterpret_cast<float *>(blk + pstep + o_re) = w * (xn.x - xs.x);
+    *reinterpret_cast<float *>(blk + pstep + o_im) = w * (xn.y - xs.y);
   }
 }
 
@@ -405,6 +419,9 @@ constexpr long ts_f2_smem_bytes(int nb) {
 
 // resident CTAs per SM asked of the register allocator: three for the
 // 384-thread shapes up to P = 24 (<= 56 registers), else whatever fits
+// the fused phase holds two row blocks and the generated program: two CTAs
+// of up to 384 threads per SM (<= 85 registers)
+#define TS_F2_PHASE_MINB(P, R) ((P) * (R) <= 384 ? 2 : 1)
 #ifndef TS_F2_MINB
 #define TS_F2_MINB(P, R) ((P) <= 24 && (P) * (R) <= 384 ? 3 : 1)
 #endif
@@ -479,7 +496,8 @@ ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
 // grid = (ceil(nlat/R) or ceil(nh/(R/2)), instances), block = P*R; shared
 // memory ts_f2_smem_bytes(max(NSYN + NGIN, NANA, 1)).
 template <class Prog, int P, int Q, int R, bool PAIRED>
-__global__ void __launch_bounds__(P *R) ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
+__global__ void __launch_bounds__(P *R, TS_F2_PHASE_MINB(P, R))
+ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
   using C = TsF2<P, Q, R>;
   constexpr int NSYN = Prog::NSYN, NGIN = Prog::NGIN, NANA = Prog::NANA, NGOUT = Prog::NGOUT;
   constexpr int NIN = NSYN + NGIN;
@@ -492,10 +510,10 @@ __global__ void __launch_bounds__(P *R) ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
   const int lat0 = blockIdx.x * (PAIRED ? R / 2 : R);
   const TsF2Rows<C, PAIRED> rows{lat0, ft.nlat, io.nh};
   ts_f2_twq<C>(twq, ft);
-#pragma unroll
+#pragma unroll 1
   for (int s = 0; s < NSYN; s++)
     ts_f2_pack<C>(buf + s * BS, io.fm + (inst * NSYN + s) * io.field, ft, rows);
-#pragma unroll
+#pragma unroll 1
   for (int gi = 0; gi < NGIN; gi++)
     ts_f2_load_rows<C>(buf + (NSYN + gi) * BS, io.gin[gi] + inst * io.gin_stride[gi], ft.nphi,
                        rows);
@@ -506,10 +524,9 @@ __global__ void __launch_bounds__(P *R) ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
   // the element-wise program: every input of a point is read before its
   // outputs overwrite the same position of the first NANA blocks
   const float *prm = io.prm + inst * io.nprm;
-  for (int i = threadIdx.x; i < C::R * C::H; i += C::T) {
-    const int r = i / C::H, n = i - r * C::H;
+  ts_f2_for_rows<C>([&](int, int r, int n) {
     const int lat = rows(r);
-    if (lat < 0) continue;
+    if (lat < 0) return;
     const int pos = r * C::RP + n;
     float in0[NIN > 0 ? NIN : 1], in1[NIN > 0 ? NIN : 1];
 #pragma unroll
@@ -527,11 +544,11 @@ __global__ void __launch_bounds__(P *R) ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
     for (int o = 0; o < NGOUT; o++)
       reinterpret_cast<float2 *>(io.gout[o] + inst * io.gout_stride[o] + (long)lat * ft.nphi)[n] =
           make_float2(out0[NANA + o], out1[NANA + o]);
-  }
+  });
   __syncthreads();
 #pragma unroll 1
   for (int k = 0; k < NANA; k++) ts_f2_forward<C>(buf + k * BS, twq);
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < NANA; k++) {
     if constexpr (PAIRED)
       ts_f2_write_w<C>(buf + k * BS, lat0, inst * NANA + k, ft, io.wq, io.wimg, io.w_nfb,
