@@ -356,6 +356,34 @@ def time_e2e(plan, q0, qa, qb, spat, B, K, stream, world, dist):
     return ems, Ke, err
 
 
+def time_imex_config1(dev, stream, precision, K=2000, graphs=True):
+    """A single Schnakenberg instance at lmax 63 on the 96 x 192 Gauss grid,
+    K steps: the launch-latency-bound case, run as captured step graphs
+    (default) or eager launches.  Returns steps/s."""
+    import torch
+    from turing_sphere_b200 import (GpuModel, ShtConfig, ShtPlan, defaultParams, mModelByKey,
+                                    seededNoise)
+    model = mModelByKey("schnakenberg")
+    plan = ShtPlan.create(dev, ShtConfig(63, 63, 96, 192), {"precision": precision})
+    gpu = GpuModel.create(dev, plan, model.source, [q.key for q in model.params], model.state,
+                          model.species, 1)
+    gpu.setGraphs(graphs)
+    gpu.setParams(defaultParams(model))
+    gpu.init(seededNoise(96 * 192, model.seedAmp, 1))
+    gpu.step(10)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    gpu.step(K)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    gpu.destroy()
+    plan.destroy()
+    return K / (ms / 1e3)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -392,11 +420,14 @@ def main():
     if args.only == "imex":
         ni = args.imex_instances
         ims, launches, ok = time_imex(dev, plan, ni, args.imex_steps, max(3, args.warmup), stream)
+        c1 = {g: time_imex_config1(dev, stream, "fp32", graphs=g) for g in (True, False)}
         if rank == 0:
             print(json.dumps({"only": "imex", "instances": ni, "launches_per_step": launches,
                               "ms_per_step": ims / args.imex_steps, "finite": ok,
                               "value": world * ni * args.imex_steps / (ims / 1e3),
-                              "unit": "instance-steps/s"}), flush=True)
+                              "unit": "instance-steps/s",
+                              "config1_steps_per_s": {"graphs": c1[True], "eager": c1[False]}}),
+                  flush=True)
         return finish(plan, plain, dev, world)
 
     q0 = np.stack([spectrum(lmax, 1000 * rank + b) for b in range(B)])
@@ -452,6 +483,8 @@ def main():
     ni = args.imex_instances
     imex_tc_ms, imex_launches, ok_tc = time_imex(dev, plan, ni, args.imex_steps, 3, stream)
     imex_fp_ms, _, ok_fp = time_imex(dev, plain, ni, max(10, args.imex_steps // 4), 3, stream)
+    c1_fp32 = time_imex_config1(dev, stream, "fp32")
+    c1_tc = time_imex_config1(dev, stream, "tf32x3")
 
     if rank == 0:
         hbm, bf16, src = measured_peaks()
@@ -505,7 +538,10 @@ def main():
                      "grid": f"lmax {lmax}, {nlat}x{nphi}", "launches_per_step": imex_launches,
                      "tc_steps_per_s": world * ni * args.imex_steps / (imex_tc_ms / 1e3),
                      "fp32_steps_per_s": world * ni * max(10, args.imex_steps // 4) / (imex_fp_ms / 1e3),
-                     "unit": "instance-steps/s", "finite": ok_tc and ok_fp},
+                     "unit": "instance-steps/s", "finite": ok_tc and ok_fp,
+                     "config1": {"workload": "1 Schnakenberg instance, lmax 63, 96x192, "
+                                             "2000 steps as captured step graphs",
+                                 "fp32_steps_per_s": c1_fp32, "tc_steps_per_s": c1_tc}},
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": sampler.summary(),

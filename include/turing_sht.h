@@ -207,6 +207,13 @@ int ts_model_upload(ts_model model, const char *name, const float *data, long n)
 int ts_model_init(ts_model model, const float *noise, long n);
 /* GpuModel.step (model.ts:229-234): `nsteps` timesteps.  Asynchronous. */
 int ts_model_step(ts_model model, int nsteps);
+/* Steps run as CUDA graphs (no reference counterpart: the reference encodes
+ * one command buffer per step, plan.ts:468-495).  After two eager warm-up
+ * steps, pairs of steps (and a single step for an odd count) are captured on
+ * the context stream once per state-buffer parity and replayed; a stream the
+ * caller is capturing itself, or the legacy default stream, runs eagerly.
+ * enable = 0 turns graphs off for this model (results are identical). */
+int ts_model_set_graphs(ts_model model, int enable);
 
 /* GpuModel.read (model.ts:262-277): blocking read of a named value — from the
  * function that ran most recently, as #locate does (model.ts:243-252).

@@ -9,7 +9,7 @@ import pytest
 
 from oracle import oracle as O
 from turing_sphere_b200 import (GpuModel, ModelSession, ShtConfig, ShtPlan, defaultParams,
-                                gridForLmax, lmIndex, mModelByKey, mModels, nlmCalc)
+                                gridForLmax, lmIndex, mModelByKey, mModels, nlmCalc, seededNoise)
 from turing_sphere_b200.registry import MModel, ParamSpec
 
 pytestmark = pytest.mark.gpu
@@ -225,6 +225,32 @@ def test_snapshot_restore_is_exact(device):
     s.gpu.restoreState()
     assert np.array_equal(s.read("U"), U)
     s.destroy()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
+def test_graph_steps_equal_eager_steps(device, precision):
+    """Steps replayed from captured CUDA graphs (pairs of steps at both state
+    parities and a single step for an odd count) give bit-identical states
+    to eagerly launched steps."""
+    model = mModelByKey("brusselator")
+    p = defaultParams(model)
+    lmax = 31
+    nlat, nphi = gridForLmax(lmax, model.pdeg)
+    sht = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi), {"precision": precision})
+    out = []
+    for graphs in (True, False):  # the context's own (capturable) stream
+        gpu = GpuModel.create(device, sht, model.source, [q.key for q in model.params],
+                              list(model.state), list(model.species), 3)
+        gpu.setGraphs(graphs)
+        gpu.setParams([dict(p, A=p["A"] + 0.1 * k) for k in range(3)])
+        gpu.init(np.concatenate([seededNoise(nlat * nphi, model.seedAmp, 7 + k)
+                                 for k in range(3)]))
+        for n in (1, 4, 3, 2, 5):  # eager warm-up, then graphs at both parities
+            gpu.step(n)
+        out.append((gpu.read("U"), gpu.read("V"), gpu.read("u")))
+        gpu.destroy()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
 
 
 def test_upload_and_read_errors(device):

@@ -102,6 +102,7 @@ SIGNATURES = {
     "ts_model_upload": (i32, [vp, cstr, f32p, i64]),
     "ts_model_init": (i32, [vp, f32p, i64]),
     "ts_model_step": (i32, [vp, i32]),
+    "ts_model_set_graphs": (i32, [vp, i32]),
     "ts_model_read": (i32, [vp, cstr, f32p, i64]),
     "ts_model_value_ptr": (i32, [vp, cstr, C.POINTER(vp), C.POINTER(i64)]),
     "ts_model_snapshot": (i32, [vp]),

@@ -170,6 +170,16 @@ struct ts_model_s {
   int last_ran = 0, stashed_ran = 0;
   std::string source;
   std::vector<float *> owned;
+  // step graphs: one or two steps captured on the context stream, keyed by
+  // the state buffers they were captured with (the ping-pong parity)
+  struct StepGraph {
+    std::vector<float *> key;
+    int nsteps;
+    cudaGraphExec_t exec;
+  };
+  std::vector<StepGraph> graphs;
+  bool use_graphs = true;
+  int eager_left = 2;  // steps run eagerly first: every lazily grown buffer exists after them
 };
 
 namespace {
@@ -770,7 +780,79 @@ void finish_shapes(ts_model m) {
     }
 }
 
+// ------------------------------------------------------------- step graphs
+
+void drop_graphs(ts_model m) {
+  for (auto &g : m->graphs) cudaGraphExecDestroy(g.exec);
+  m->graphs.clear();
+}
+
+// Graphs need a stream that can be captured and is not being captured by
+// the caller already (a caller's capture records the eager launches).
+bool graphs_usable(ts_model m) {
+  if (!m->use_graphs) return false;
+  cudaStream_t st = m->ctx->stream;
+  if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) return false;
+  cudaStreamCaptureStatus cs;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return false;
+  return cs == cudaStreamCaptureStatusNone;
+}
+
+std::vector<float *> state_key(ts_model m) {
+  std::vector<float *> k;
+  for (auto &name : m->prog[1].swaps) k.push_back(m->host.at(name).cur);
+  return k;
+}
+
+void swap_states(ts_model m, int nsteps) {
+  for (int i = 0; i < nsteps; i++)
+    for (auto &name : m->prog[1].swaps) {
+      HostBuf &h = m->host.at(name);
+      std::swap(h.cur, h.next);
+    }
+}
+
+// nsteps steps as one graph launch; the graph for the current state
+// buffers is captured on first use.  Any capture failure turns graphs off
+// for the model and runs the steps eagerly.
+void run_steps_graphed(ts_model m, int nsteps) {
+  cudaStream_t st = m->ctx->stream;
+  const std::vector<float *> key = state_key(m);
+  for (auto &g : m->graphs)
+    if (g.nsteps == nsteps && g.key == key) {
+      TS_CUDA(cudaGraphLaunch(g.exec, st));
+      swap_states(m, nsteps);
+      return;
+    }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    int ran = 0;
+    try {
+      for (; ran < nsteps; ran++) run_program(m, m->prog[1], st);
+    } catch (const ts_exc &) {
+      ok = false;
+    }
+    const bool ended = cudaStreamEndCapture(st, &graph) == cudaSuccess;
+    ok = ok && ended && graph;
+    if (!ok) swap_states(m, ran);  // undo the host-side swaps of the failed capture
+  }
+  if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok) {
+    (void)cudaGetLastError();
+    m->use_graphs = false;
+    drop_graphs(m);
+    for (int i = 0; i < nsteps; i++) run_program(m, m->prog[1], st);
+    return;
+  }
+  m->graphs.push_back({key, nsteps, exec});
+  TS_CUDA(cudaGraphLaunch(exec, st));
+}
+
 void free_model(ts_model m) {
+  drop_graphs(m);
   for (auto &kv : m->host) {
     if (kv.second.cur) cudaFree(kv.second.cur);
     if (kv.second.next) cudaFree(kv.second.next);
@@ -1044,8 +1126,24 @@ int ts_model_init(ts_model m, const float *noise, long n) {
 int ts_model_step(ts_model m, int nsteps) {
   TSM_BEGIN(m)
   TS_REQUIRE(nsteps >= 0, TS_ERR_INVALID, "nsteps must be >= 0");
-  for (int i = 0; i < nsteps; i++) run_program(m, m->prog[1], ctx->stream);
+  int done = 0;
+  for (; done < nsteps && (m->eager_left > 0 || !graphs_usable(m)); done++) {
+    run_program(m, m->prog[1], ctx->stream);
+    if (m->eager_left > 0) m->eager_left--;
+  }
+  while (nsteps - done >= 2) {
+    run_steps_graphed(m, 2);
+    done += 2;
+  }
+  if (done < nsteps) run_steps_graphed(m, 1);
   if (nsteps > 0) m->last_ran = 1;
+  TSM_END
+}
+
+int ts_model_set_graphs(ts_model m, int enable) {
+  TSM_BEGIN(m)
+  m->use_graphs = enable != 0;
+  drop_graphs(m);
   TSM_END
 }
 

@@ -115,6 +115,10 @@ class GpuModel:
     def step(self, steps: int = 1) -> None:
         self._check(_lib.lib().ts_model_step(self.handle, steps))
 
+    def setGraphs(self, enable: bool) -> None:
+        """Run steps as captured CUDA graphs (default) or launch them eagerly."""
+        self._check(_lib.lib().ts_model_set_graphs(self.handle, 1 if enable else 0))
+
     def snapshotState(self) -> None:
         self._check(_lib.lib().ts_model_snapshot(self.handle))
 
