@@ -413,8 +413,8 @@ def main():
     torch.cuda.set_stream(stream)
     dev.set_stream(stream.cuda_stream)
     cfg = ShtConfig(lmax, lmax, nlat, nphi)
-    plan = ShtPlan.create(dev, cfg, {"precision": args.precision})
-    plain = ShtPlan.create(dev, cfg, {"precision": "fp32"})
+    plan = ShtPlan.create(dev, cfg, {"precision": args.precision, "autotune": True})
+    plain = ShtPlan.create(dev, cfg, {"precision": "fp32", "autotune": True})
     nlm = plan.nlm
 
     if args.only == "imex":
@@ -471,6 +471,7 @@ def main():
     if args.only == "sht":
         if rank == 0:
             print(json.dumps({"only": "sht", "ms_per_step": ms / K, "stage_ms": stage_ms,
+                              "kernel_shapes": plan.shapes,
                               "value": world * B * K / (ms / 1e3), "unit": "SHT pairs/s"}),
                   flush=True)
         return finish(plan, plain, dev, world)
@@ -526,7 +527,8 @@ def main():
             "config": {"workload": f"batched SHT round trip (synth+analys), lmax=mmax={lmax}, "
                                    f"{nlat}x{nphi} Gauss grid, B={B} fields per GPU",
                        "precision": args.precision, "fourier": plan.fourierMode,
-                       "fft_radices": plan.fftRadices, "global_batch": B * world,
+                       "fft_radices": plan.fftRadices, "kernel_shapes": plan.shapes,
+                       "global_batch": B * world,
                        "l2": f"inputs larger than L2 (grid fields {sp_b / 1e6:.0f} MB/step)"},
             "e2e": {"value": world * B * Ke / (ems / 1e3), "unit": "SHT pairs/s",
                     "h2d_bytes_per_step": int(nlm_b), "d2h_bytes_per_step": int(nlm_b),

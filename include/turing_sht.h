@@ -59,7 +59,8 @@ enum ts_plan_flags {
   TS_FOURIER_AUTO = 0,     /* mixed-radix FFT whenever nphi = 2^a 3^b, else DFT */
   TS_FOURIER_FFT = 0x10,   /* require the FFT (error if nphi has other factors) */
   TS_FOURIER_DFT = 0x20,   /* direct band-limited sum (sht.ts:241-289 semantics) */
-  TS_FOURIER_MASK = 0x30
+  TS_FOURIER_MASK = 0x30,
+  TS_PLAN_AUTOTUNE = 0x40  /* time the kernel shapes at plan creation, keep the fastest */
 };
 
 /* ------------------------------------------------------------ context
@@ -102,6 +103,12 @@ typedef struct ts_plan_info {
   int fft_stages; /* Stockham stages of the nphi/2-point FFT (0 for DFT) */
   int fft_radix[16];
   long table_bytes; /* tensor-core P tables in device memory (0 for FP32) */
+  /* kernel shapes in use (chosen by TS_PLAN_AUTOTUNE, else the defaults) */
+  int tc_lat_tile;   /* tensor-core synthesis: latitudes per tile (0 for FP32) */
+  int tc_deg_tile;   /* tensor-core analysis: degrees per tile (0 for FP32) */
+  int fft_p, fft_q;  /* two-phase FFT H = P*Q (0 when the Stockham/DFT kernels run) */
+  int fft_rows;      /* grid rows per FFT CTA */
+  int tuned;         /* 1 when the shapes were timed (TS_PLAN_AUTOTUNE) */
 } ts_plan_info;
 int ts_sht_plan_info(ts_plan plan, ts_plan_info *info);
 

@@ -102,3 +102,26 @@ def test_w_stages_equal_analys_dev(device):
     from turing_sphere_b200._lib import TsError
     with pytest.raises(TsError):
         plain.stage_dev("fourAnalysW", spat.data_ptr(), img.data_ptr(), B)
+
+
+def test_autotuned_plan_keeps_parity(device):
+    """TS_PLAN_AUTOTUNE times the tensor-core tiles and the FFT rows per CTA,
+    keeps the fastest (reported in `shapes`) and stays within 1e-5; a second
+    plan of the same grid reuses the choice."""
+    lmax, nlat, nphi = 127, 192, 384
+    cfg = ShtConfig(lmax, lmax, nlat, nphi)
+    plan = ShtPlan.create(device, cfg, {"precision": "tf32x3", "autotune": True})
+    sh = plan.shapes
+    assert sh["tuned"] and sh["tc_lat_tile"] in (64, 96) and sh["tc_deg_tile"] in (64, 128)
+    assert (sh["fft_p"], sh["fft_q"]) == (16, 12) and sh["fft_rows"] in (8, 16)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = scaled_spectrum(lmax, lmax, 31)
+    s_cpu = ref.synth(q.astype(np.float64))
+    assert O.rel_l2(plan.synth(q), s_cpu) < TOL
+    s32 = s_cpu.astype(np.float32)
+    assert O.rel_l2(plan.analys(s32), ref.analys(s32.astype(np.float64))) < TOL
+    plan.status()
+    again = ShtPlan.create(device, cfg, {"precision": "tf32x3", "autotune": True})
+    assert again.shapes == sh
+    default = tc_plan(device, lmax, nlat, nphi)
+    assert not default.shapes["tuned"] and default.shapes["tc_lat_tile"] == 96

@@ -28,6 +28,7 @@ TS_PREC_BF16X3 = 2
 TS_FOURIER_AUTO = 0
 TS_FOURIER_FFT = 0x10
 TS_FOURIER_DFT = 0x20
+TS_PLAN_AUTOTUNE = 0x40
 
 STATUS_NAMES = {
     TS_ERR_INVALID: "invalid", TS_ERR_CUDA: "cuda", TS_ERR_COMPILE: "compile",
@@ -49,6 +50,8 @@ class PlanInfo(C.Structure):
         ("lmax", C.c_int), ("mmax", C.c_int), ("nlat", C.c_int), ("nphi", C.c_int),
         ("nlm", C.c_long), ("precision", C.c_int), ("fourier", C.c_int),
         ("fft_stages", C.c_int), ("fft_radix", C.c_int * 16), ("table_bytes", C.c_long),
+        ("tc_lat_tile", C.c_int), ("tc_deg_tile", C.c_int), ("fft_p", C.c_int),
+        ("fft_q", C.c_int), ("fft_rows", C.c_int), ("tuned", C.c_int),
     ]
 
 

@@ -260,6 +260,7 @@ int ts_sht_plan_create(ts_ctx ctx, int lmax, int mmax, int nlat, int nphi, int f
     if (p->precision == TS_PREC_BF16X3)
       ts_throw(TS_ERR_UNSUPPORTED, "split-BF16 tensor-core Legendre is not built; use TF32x3");
     if (p->precision == TS_PREC_TF32X3) ts_tc_init(p);
+    if (flags & TS_PLAN_AUTOTUNE) ts_autotune(p);
     *out = p;
     return TS_OK;
   } catch (const ts_exc &e) {
@@ -294,6 +295,18 @@ int ts_sht_plan_info(ts_plan p, ts_plan_info *info) {
   info->fft_stages = p->fourier == TS_FOURIER_FFT ? p->fft.nst : 0;
   info->table_bytes = (long)ts_tc_bytes(p);
   for (int i = 0; i < info->fft_stages; i++) info->fft_radix[i] = p->fft.radix[i];
+  if (p->tc) {
+    const TsTcGeom g = ts_tc_geom(p);
+    info->tc_lat_tile = g.NL;
+    info->tc_deg_tile = g.LTL;
+  }
+  int P = 0, Q = 0;
+  if (ts_f2_shape(p, &P, &Q)) {
+    info->fft_p = P;
+    info->fft_q = Q;
+    info->fft_rows = ts_f2_rows(p);
+  }
+  info->tuned = p->tuned ? 1 : 0;
   return TS_OK;
 }
 

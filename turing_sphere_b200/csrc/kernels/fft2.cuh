@@ -417,14 +417,12 @@ constexpr long ts_f2_smem_bytes(int nb) {
 
 // ---------------------------------------------------------------- kernels
 
-// resident CTAs per SM asked of the register allocator: three for the
-// 384-thread shapes up to P = 24 (<= 56 registers), else whatever fits
-// the fused phase holds two row blocks and the generated program: two CTAs
-// of up to 384 threads per SM (<= 85 registers)
+// Resident CTAs per SM asked of the register allocator.  Transform kernels
+// with P <= 24: 1152 threads per SM (<= 56 registers each), else whatever
+// fits.  The fused phase holds two row blocks and the generated program: two
+// CTAs of up to 384 threads per SM (<= 85 registers).
+#define TS_F2_MINB(P, R) ((P) <= 24 ? 1152 / ((P) * (R)) : 1)
 #define TS_F2_PHASE_MINB(P, R) ((P) * (R) <= 384 ? 2 : 1)
-#ifndef TS_F2_MINB
-#define TS_F2_MINB(P, R) ((P) <= 24 && (P) * (R) <= 384 ? 3 : 1)
-#endif
 
 // fm[field][m][lat] -> spat[field][lat][phi].  grid = (ceil(nlat/R), fields),
 // block = P*R.

@@ -77,7 +77,15 @@ struct ts_plan_s {
   ts_dbuf fm, stage_q, stage_s;
   // tensor-core tables (precision != FP32)
   void *tc = nullptr;
+  // kernel shapes: 0 = default (or TS_TC_NL / TS_TC_LTL); set by the autotuner
+  int tune_nl = 0, tune_ltl = 0, fft_rows = 0;
+  bool tuned = false;
 };
+
+// autotune.cu: time the candidate kernel shapes of a plan, keep the fastest
+void ts_autotune(ts_plan p);
+// rows per two-phase FFT CTA in use (0 when the plan's rows have no shape)
+int ts_f2_rows(ts_plan p);
 
 cudaStream_t ts_pick_stream(ts_ctx ctx, void *stream);
 void ts_set_error(ts_ctx ctx, const std::string &msg);

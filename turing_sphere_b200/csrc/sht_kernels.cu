@@ -373,28 +373,29 @@ void ts_launch_leg_analys(ts_plan p, const float2 *g, long gs, float2 *q, long q
 }
 
 // Two-phase FFT shapes: H = P*Q with P, Q in-register DFT lengths, and the
-// rows R of a transform CTA (P*R threads)
+// two row counts R of a transform CTA (P*R threads) the kernels are built
+// for: X(H, P, Q, R_small, R_default)
 #define TS_F2_SHAPES(X) \
-  X(32, 8, 4, 16)       \
-  X(48, 8, 6, 16)       \
-  X(64, 8, 8, 16)       \
-  X(96, 12, 8, 16)      \
-  X(128, 16, 8, 16)     \
-  X(192, 16, 12, 16)    \
-  X(256, 16, 16, 16)    \
-  X(384, 24, 16, 16)    \
-  X(512, 32, 16, 16)    \
-  X(768, 32, 24, 16)    \
-  X(1024, 32, 32, 16)   \
-  X(1536, 48, 32, 8)
+  X(32, 8, 4, 8, 16)    \
+  X(48, 8, 6, 8, 16)    \
+  X(64, 8, 8, 8, 16)    \
+  X(96, 12, 8, 8, 16)   \
+  X(128, 16, 8, 8, 16)  \
+  X(192, 16, 12, 8, 16) \
+  X(256, 16, 16, 8, 16) \
+  X(384, 24, 16, 8, 16) \
+  X(512, 32, 16, 8, 16) \
+  X(768, 32, 24, 8, 16) \
+  X(1024, 32, 32, 8, 16) \
+  X(1536, 48, 32, 4, 8)
 
 bool ts_f2_shape(ts_plan p, int *P, int *Q) {
   if (p->fourier != TS_FOURIER_FFT) return false;
   switch (p->fft.H) {
-#define TS_F2_CASE(h, pp, qq, rr) \
-  case h:                         \
-    *P = pp;                      \
-    *Q = qq;                      \
+#define TS_F2_CASE(h, pp, qq, rlo, rhi) \
+  case h:                               \
+    *P = pp;                            \
+    *Q = qq;                            \
     return true;
     TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
@@ -464,13 +465,29 @@ void f2_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb, char *w
 }
 }  // namespace
 
+int ts_f2_rows(ts_plan p) {
+  if (p->fourier != TS_FOURIER_FFT) return 0;
+  switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rlo, rhi) \
+  case h:                               \
+    return p->fft_rows == rlo ? rlo : rhi;
+    TS_F2_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+    default:
+      return 0;
+  }
+}
+
 bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb,
                                 char *wimg, cudaStream_t s) {
   if (p->fourier != TS_FOURIER_FFT) return false;
   switch (p->fft.H) {
-#define TS_F2_CASE(h, pp, qq, rr) \
-  case h:                         \
-    f2_analys_w<pp, qq, rr>(p, spat, ss, nf, fpb, wimg, s); \
+#define TS_F2_CASE(h, pp, qq, rlo, rhi)                                     \
+  case h:                                                                   \
+    if (p->fft_rows == rlo)                                                 \
+      f2_analys_w<pp, qq, rlo>(p, spat, ss, nf, fpb, wimg, s);              \
+    else                                                                    \
+      f2_analys_w<pp, qq, rhi>(p, spat, ss, nf, fpb, wimg, s);              \
     return true;
     TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
@@ -483,9 +500,10 @@ void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, 
                              cudaStream_t s) {
   if (p->fourier == TS_FOURIER_FFT) {
     switch (p->fft.H) {
-#define TS_F2_CASE(h, pp, qq, rr) \
-  case h:                         \
-    return f2_synth<pp, qq, rr>(p, fm, fs, spat, ss, nf, s);
+#define TS_F2_CASE(h, pp, qq, rlo, rhi)                                         \
+  case h:                                                                       \
+    return p->fft_rows == rlo ? f2_synth<pp, qq, rlo>(p, fm, fs, spat, ss, nf, s) \
+                              : f2_synth<pp, qq, rhi>(p, fm, fs, spat, ss, nf, s);
       TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
       default:
@@ -509,9 +527,10 @@ void ts_launch_fourier_analys(ts_plan p, const float *spat, long ss, float2 *g, 
                               cudaStream_t s) {
   if (p->fourier == TS_FOURIER_FFT) {
     switch (p->fft.H) {
-#define TS_F2_CASE(h, pp, qq, rr) \
-  case h:                         \
-    return f2_analys<pp, qq, rr>(p, spat, ss, g, gs, nf, s);
+#define TS_F2_CASE(h, pp, qq, rlo, rhi)                                        \
+  case h:                                                                      \
+    return p->fft_rows == rlo ? f2_analys<pp, qq, rlo>(p, spat, ss, g, gs, nf, s) \
+                              : f2_analys<pp, qq, rhi>(p, spat, ss, g, gs, nf, s);
       TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
       default:

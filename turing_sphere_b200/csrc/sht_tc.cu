@@ -96,16 +96,23 @@ int kpar_h(int lmax, int m, int par) { return (lmax - m + 1 + 1 - par) / 2; }
 // Tile geometry of the tensor-core kernels, from the plan's sizes alone (so
 // the model compiler can size shared memory without the tables).  TS_TC_NL
 // (the synthesis latitude tile, a multiple of 16 <= 128) and TS_TC_LTL (the
-// analysis degree tile, a multiple of 16 <= 256) tune it, like the
+// analysis degree tile, a multiple of 16 <= 128: two 256-column accumulator
+// buffers) tune it, like the
 // reference's SHT_* knobs (src/sht/sht.ts:47-56).
 TsTcGeom ts_tc_geom(ts_plan p) {
   TsTcGeom g;
   int nl_cap = 96;  // two accumulator buffers of 2*NL columns fit in 512
-  if (const char *e = getenv("TS_TC_NL")) nl_cap = std::max(16, std::min(128, atoi(e) & ~15));
+  if (p->tune_nl > 0)
+    nl_cap = std::max(16, std::min(128, p->tune_nl & ~15));
+  else if (const char *e = getenv("TS_TC_NL"))
+    nl_cap = std::max(16, std::min(128, atoi(e) & ~15));
   g.NL = std::min(nl_cap, ((p->nh + 15) / 16) * 16);
   g.nLT = (p->nh + g.NL - 1) / g.NL;
   g.LTL = 128;
-  if (const char *e = getenv("TS_TC_LTL")) g.LTL = std::max(16, std::min(256, atoi(e) & ~15));
+  if (p->tune_ltl > 0)
+    g.LTL = std::max(16, std::min(128, p->tune_ltl & ~15));
+  else if (const char *e = getenv("TS_TC_LTL"))
+    g.LTL = std::max(16, std::min(128, atoi(e) & ~15));
   g.ntile = (kpar_h(p->lmax, 0, 0) + g.LTL - 1) / g.LTL;
   return g;
 }

@@ -83,6 +83,10 @@ class ShtPlan:
         self.precision = {v: k for k, v in PRECISIONS.items()}[info.precision]
         self.fftRadices = [info.fft_radix[i] for i in range(info.fft_stages)]
         self.tableBytes = info.table_bytes
+        # kernel shapes in use: tensor-core tiles, two-phase FFT split, FFT rows per CTA
+        self.shapes = {"tc_lat_tile": info.tc_lat_tile, "tc_deg_tile": info.tc_deg_tile,
+                       "fft_p": info.fft_p, "fft_q": info.fft_q, "fft_rows": info.fft_rows,
+                       "tuned": bool(info.tuned)}
         x = np.zeros(cfg.nlat)
         w = np.zeros(cfg.nlat)
         _lib.check(_lib.lib().ts_sht_plan_nodes(handle, _lib.dptr(x), _lib.dptr(w)), device.handle)
@@ -94,10 +98,13 @@ class ShtPlan:
     @staticmethod
     def create(device: Device, cfg: ShtConfig, opts: dict | None = None) -> "ShtPlan":
         """ShtPlan.create (sht.ts:166-183).  opts: fourier = auto|fft|dft,
-        precision = fp32|tf32x3|bf16x3."""
+        precision = fp32|tf32x3|bf16x3, autotune = True to time the kernel
+        shapes at creation (the choice is in `shapes`)."""
         opts = opts or {}
         validateConfig(cfg)
         flags = PRECISIONS[opts.get("precision", "fp32")] | FOURIERS[opts.get("fourier", "auto")]
+        if opts.get("autotune"):
+            flags |= _lib.TS_PLAN_AUTOTUNE
         h = C.c_void_p()
         rc = _lib.lib().ts_sht_plan_create(device.handle, cfg.lmax, cfg.mmax, cfg.nlat, cfg.nphi,
                                            flags, C.byref(h))
