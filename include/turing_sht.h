@@ -56,6 +56,7 @@ enum ts_plan_flags {
   TS_PREC_BF16X3 = 2,      /* tcgen05 tensor-core Legendre, 3-pass split BF16 */
   TS_PREC_MASK = 0xF,
   TS_CHECK_SOURCE = 0x100, /* ts_model_check: return the generated source */
+  TS_CHECK_ADJOINT = 0x200, /* ts_model_check: also generate and compile the step's adjoint */
   TS_FOURIER_AUTO = 0,     /* mixed-radix FFT whenever nphi = 2^a 3^b, else DFT */
   TS_FOURIER_FFT = 0x10,   /* require the FFT (error if nphi has other factors) */
   TS_FOURIER_DFT = 0x20,   /* direct band-limited sum (sht.ts:241-289 semantics) */
@@ -159,6 +160,17 @@ int ts_sht_fourier_analys_dev(ts_plan plan, const float *spat, float *fm, int ba
                               void *stream);
 int ts_sht_leg_analys_dev(ts_plan plan, const float *fm, float *qlm, int batch, void *stream);
 
+/* Adjoints of the transforms (no reference counterpart: the reference has
+ * no differentiation).  With coefficients read as 2*nlm reals and the grid
+ * as nlat*nphi reals, synth_adjoint applies S^T (grid cotangent -> spectral
+ * cotangent) and analys_adjoint applies A^T (spectral -> grid), exactly the
+ * transposes of ts_sht_synth_dev / ts_sht_analys_dev; the imaginary part of
+ * m = 0 of a spectral cotangent is zero. */
+int ts_sht_synth_adjoint_dev(ts_plan plan, const float *gbar, float *qbar, int batch,
+                             void *stream);
+int ts_sht_analys_adjoint_dev(ts_plan plan, const float *qbar, float *gbar, int batch,
+                              void *stream);
+
 /* The two stages of ts_sht_analys_dev on a tensor-core plan, for timing them
  * apart (no reference counterpart: the reference has one analysis path).  The
  * Fourier analysis writes the folded, weighted operand image of the
@@ -221,6 +233,19 @@ int ts_model_step(ts_model model, int nsteps);
  * caller is capturing itself, or the legacy default stream, runs eagerly.
  * enable = 0 turns graphs off for this model (results are identical). */
 int ts_model_set_graphs(ts_model model, int enable);
+
+/* Forward/backward pair of the adjoint (no reference counterpart; the
+ * autograd.Function of this path).  Advances the model nsteps steps from its
+ * current state, as ts_model_step does, keeping a checkpoint of the state
+ * every `every` steps; then runs the hand-written adjoint of the step (the
+ * transposed transforms, the symbolically differentiated element-wise
+ * statements and the implicit diffusion solve) backwards, replaying each
+ * segment from its checkpoint.  final_bar: dL/d(final state), host
+ * [state][instance][2 nlm] in the model's state order; init_bar receives
+ * dL/d(initial state) in the same layout; param_bar (may be NULL) receives
+ * dL/d(parameters), host double [instance][nparams]. */
+int ts_model_forward_backward(ts_model model, int nsteps, int every, const float *final_bar,
+                              float *init_bar, double *param_bar);
 
 /* GpuModel.read (model.ts:262-277): blocking read of a named value — from the
  * function that ran most recently, as #locate does (model.ts:243-252).

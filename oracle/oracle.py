@@ -168,6 +168,21 @@ class ShtReference:
     def analys(self, spat):
         return self._run("ors_analys", spat, 2 * self.nlm)
 
+    def synth_adjoint(self, gbar):
+        """S^T gbar, the transpose of synth with coefficients read as 2*nlm
+        reals: c_m * analys(gbar / (w_i 2 pi/nphi)), c_0 = 1, c_m = 2 (a real
+        field from its m >= 0 half), m = 0 imaginary parts zero.  Test
+        helper for the adjoint's losses."""
+        g = np.asarray(gbar, dtype=np.float64).reshape(self.nlat, self.nphi)
+        q = self.analys((g / (self.wg[:, None] * (2 * np.pi / self.nphi))).ravel())
+        if not hasattr(self, "_c"):
+            c = np.full(2 * self.nlm, 2.0)
+            for l in range(self.lmax + 1):
+                i = lm_index(self.lmax, l, 0)
+                c[2 * i], c[2 * i + 1] = 1.0, 0.0
+            self._c = c
+        return q * self._c
+
     def model_step(self, model: str, params, state, nsteps: int):
         """Advance ``state`` (species x 2*nlm, f64) by ``nsteps`` IMEX steps."""
         mid = MODELS[model]

@@ -56,6 +56,33 @@ def test_schnakenberg_compiles_on_large_grids(grid, precision):
 
 
 LINEAR = open(__file__.replace("test_mcompile.py", "models/linear.m")).read()
+LOGISTIC = open(__file__.replace("test_mcompile.py", "models/logistic.m")).read()
+
+
+@pytest.mark.parametrize("which", ["schnakenberg", "brusselator", "allencahn", "linear",
+                                   "logistic"])
+def test_step_adjoint_generates_and_compiles(which):
+    """TS_CHECK_ADJOINT: the reverse-mode kernels of every model's step
+    (symbolic derivatives of its element-wise statements) compile for
+    sm_100a; the IMEX update's parameter derivatives are emitted."""
+    if which in ("linear", "logistic"):
+        src = LINEAR if which == "linear" else LOGISTIC
+        params = ["c", "D", "dt"] if which == "linear" else ["r", "D", "dt"]
+        state, view = ("U",), ("u",)
+    else:
+        m = [x for x in mModels if x.key == which][0]
+        src, params, state, view = m.source, [p.key for p in m.params], m.state, m.species
+    buf = C.create_string_buffer(1 << 20)
+    k, n = C.c_int(), C.c_int()
+    err = _lib.CompileError()
+    rc = _lib.lib().ts_model_check(31, 31, 48, 96, src.encode(), _lib.cstr_array(list(state)),
+                                   len(state), _lib.cstr_array(list(view)), len(view),
+                                   _lib.cstr_array(list(params)), len(params), 4,
+                                   _lib.TS_CHECK_SOURCE | _lib.TS_CHECK_ADJOINT, buf, len(buf),
+                                   C.byref(k), C.byref(n), C.byref(err))
+    assert rc == _lib.TS_OK, err.message.decode()
+    code = buf.value.decode()
+    assert "ts_adj_r0" in code and "atomicAdd(io.pbar" in code
 
 
 @pytest.mark.parametrize("src,msg", [

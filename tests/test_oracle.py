@@ -120,3 +120,18 @@ def test_oracle_reaction_matches_spec_h():
         assert np.allclose(r1, np.array(e["r1"]), rtol=1e-6, atol=1e-6)
         if r2 is not None:
             assert np.allclose(r2, np.array(e["r2"]), rtol=1e-6, atol=1e-6)
+
+
+def test_oracle_synth_adjoint_is_the_transpose():
+    """<synth q, g> = <q, synth_adjoint g> in f64 (the helper the adjoint
+    tests form their grid-loss cotangents with)."""
+    lmax, nlat, nphi = 15, 24, 48
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    rng = np.random.default_rng(3)
+    q = rng.standard_normal(2 * ref.nlm)
+    for l in range(lmax + 1):
+        q[2 * O.lm_index(lmax, l, 0) + 1] = 0.0
+    g = rng.standard_normal(nlat * nphi)
+    lhs = float(np.dot(ref.synth(q), g))
+    rhs = float(np.dot(q, ref.synth_adjoint(g)))
+    assert abs(lhs - rhs) < 1e-10 * max(1.0, abs(lhs))

@@ -190,3 +190,34 @@ def test_errors(device):
         make(device, 31, 32, 100, fourier="fft")
     with pytest.raises(ValueError, match="nlat must be"):
         make(device, 31, 31, 64)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
+@pytest.mark.parametrize("lmax,nlat,nphi", [(31, 32, 64), (63, 96, 192), (20, 33, 64)])
+def test_transform_adjoints_dot_product(device, precision, lmax, nlat, nphi):
+    """<synth q, g> = <q, synth^T g> and <analys g, q> = <g, analys^T q> for
+    random q (m = 0 imaginary parts zero) and g, batch 2 (odd nlat: the
+    equator row counts once)."""
+    import torch
+    plan = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi), {"precision": precision})
+    B, nlm = 2, plan.nlm
+    rng = np.random.default_rng(lmax)
+    q = np.stack([scaled_spectrum(lmax, lmax, 50 + b) for b in range(B)])
+    g = rng.standard_normal((B, nlat * nphi)).astype(np.float32)
+    qd, gd = torch.from_numpy(q).cuda(), torch.from_numpy(g).cuda()
+    Sq, STg = torch.empty_like(gd), torch.empty_like(qd)
+    Ag, ATq = torch.empty_like(qd), torch.empty_like(gd)
+    plan.synth_dev(qd.data_ptr(), Sq.data_ptr(), B)
+    plan.synth_adjoint_dev(gd.data_ptr(), STg.data_ptr(), B)
+    plan.analys_dev(gd.data_ptr(), Ag.data_ptr(), B)
+    plan.analys_adjoint_dev(qd.data_ptr(), ATq.data_ptr(), B)
+    torch.cuda.synchronize()
+    plan.status()
+    d = lambda a, b: float((a.double() * b.double()).sum())
+    l1, r1 = d(Sq, gd), d(qd, STg)
+    l2, r2 = d(Ag, qd), d(gd, ATq)
+    assert abs(l1 - r1) <= 1e-5 * (abs(l1) + float(Sq.double().norm() * gd.double().norm()) * 1e-2)
+    assert abs(l2 - r2) <= 1e-5 * (abs(l2) + float(Ag.double().norm() * qd.double().norm()) * 1e-2)
+    # m = 0 imaginary parts of the spectral cotangent are zero
+    idx = [2 * i + 1 for i in range(lmax + 1)]  # m = 0 block, imaginary
+    assert float(STg[:, idx].abs().max()) == 0.0

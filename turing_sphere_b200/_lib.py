@@ -29,6 +29,8 @@ TS_FOURIER_AUTO = 0
 TS_FOURIER_FFT = 0x10
 TS_FOURIER_DFT = 0x20
 TS_PLAN_AUTOTUNE = 0x40
+TS_CHECK_SOURCE = 0x100
+TS_CHECK_ADJOINT = 0x200
 
 STATUS_NAMES = {
     TS_ERR_INVALID: "invalid", TS_ERR_CUDA: "cuda", TS_ERR_COMPILE: "compile",
@@ -95,6 +97,8 @@ SIGNATURES = {
     "ts_sht_fourier_analys_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_leg_analys_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_wimage_bytes": (C.c_size_t, [vp, i32]),
+    "ts_sht_synth_adjoint_dev": (i32, [vp, vp, vp, i32, vp]),
+    "ts_sht_analys_adjoint_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_fourier_analys_w_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_leg_analys_w_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_model_compile": (i32, [vp, cstr, C.POINTER(cstr), i32, C.POINTER(cstr), i32,
@@ -106,6 +110,7 @@ SIGNATURES = {
     "ts_model_init": (i32, [vp, f32p, i64]),
     "ts_model_step": (i32, [vp, i32]),
     "ts_model_set_graphs": (i32, [vp, i32]),
+    "ts_model_forward_backward": (i32, [vp, i32, i32, f32p, f32p, f64p]),
     "ts_model_read": (i32, [vp, cstr, f32p, i64]),
     "ts_model_value_ptr": (i32, [vp, cstr, C.POINTER(vp), C.POINTER(i64)]),
     "ts_model_snapshot": (i32, [vp]),

@@ -84,6 +84,8 @@ void plan_free(ts_plan p) {
   p->fm.release();
   p->stage_q.release();
   p->stage_s.release();
+  p->adj_grid.release();
+  p->adj_spec.release();
   ts_tc_free(p);
 }
 
@@ -95,7 +97,9 @@ void check_batch(ts_plan p, const void *a, const void *b, int batch) {
 
 long npts_of(ts_plan p) { return (long)p->nlat * p->nphi; }
 
-void synth_dev(ts_plan p, const float *qlm, float *spat, int batch, cudaStream_t s) {
+}  // namespace
+
+void ts_synth_dev(ts_plan p, const float *qlm, float *spat, int batch, cudaStream_t s) {
   const long fm_stride = (long)(p->mmax + 1) * p->nlat;
   p->fm.ensure(sizeof(float2) * fm_stride * batch);
   float2 *fm = (float2 *)p->fm.p;
@@ -103,7 +107,7 @@ void synth_dev(ts_plan p, const float *qlm, float *spat, int batch, cudaStream_t
   ts_launch_fourier_synth(p, fm, fm_stride, spat, npts_of(p), batch, s);
 }
 
-void analys_dev(ts_plan p, const float *spat, float *qlm, int batch, cudaStream_t s) {
+void ts_analys_dev(ts_plan p, const float *spat, float *qlm, int batch, cudaStream_t s) {
   if (p->precision != TS_PREC_FP32) return ts_analys_tc_full(p, spat, npts_of(p), qlm, batch, s);
   const long fm_stride = (long)(p->mmax + 1) * p->nlat;
   p->fm.ensure(sizeof(float2) * fm_stride * batch);
@@ -112,6 +116,13 @@ void analys_dev(ts_plan p, const float *spat, float *qlm, int batch, cudaStream_
   ts_launch_leg_analys(p, fm, fm_stride, (float2 *)qlm, p->nlm, batch, s);
 }
 
+namespace {
+void synth_dev(ts_plan p, const float *qlm, float *spat, int batch, cudaStream_t s) {
+  ts_synth_dev(p, qlm, spat, batch, s);
+}
+void analys_dev(ts_plan p, const float *spat, float *qlm, int batch, cudaStream_t s) {
+  ts_analys_dev(p, spat, qlm, batch, s);
+}
 }  // namespace
 
 void ts_set_error(ts_ctx ctx, const std::string &msg) {

@@ -18,6 +18,9 @@
 #define TS_ACCURACY 1e-15f
 #define TS_RESCALE_THR (TS_ACCURACY * TS_SCALE + 1.0f)
 
+// a >= b ? x : y (derivatives of max/min in generated adjoint code)
+TS_DEV float ts_ge_sel(float a, float b, float x, float y) { return a >= b ? x : y; }
+
 TS_DEV float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 TS_DEV float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 TS_DEV float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
@@ -145,6 +148,26 @@ struct TsPhaseIO {
   char *wimg;
   int w_nfb, w_fpb, w_nlc, nh;
   const float *wq;
+};
+
+// I/O of a model's generated adjoint kernels: the forward ("tape") kernel of
+// an element-wise statement reads its inputs in[] and writes out; the
+// reverse kernel reads the inputs and the output cotangent gout, adds the
+// input cotangents into gin[] and the parameter gradients into pbar
+// ([instance][nprm], double).  Strides are per instance (0 = shared).
+struct TsAdjIO {
+  const float *in[TS_MAXIO];
+  long in_stride[TS_MAXIO];
+  float *out;
+  long out_stride;
+  const float *gout;
+  long gout_stride;
+  float *gin[TS_MAXIO];
+  long gin_stride[TS_MAXIO];
+  const float *prm;
+  int nprm;
+  double *pbar;
+  long n;  // elements per instance
 };
 
 // Spectral-side I/O of a compiled model's generated code: inputs and outputs

@@ -121,4 +121,14 @@ Function specialize(const std::vector<AstFunction> &file, const std::string &nam
 std::string describe(const Function &f);
 int count_kernels(const Function &f);
 
+// Symbolic derivative d e / d w (mdiff.cpp): w is a variable or a model
+// parameter slot; derived scalars are differentiated through.  The result
+// may call "__ge_sel"(a, b, x, y) = a >= b ? x : y (max/min).
+struct Wrt {
+  enum Kind { Var, Param } kind;
+  int index;
+};
+ExprP differentiate(const Function &f, const ExprP &e, const Wrt &w);
+bool is_zero(const ExprP &e);
+
 }  // namespace tsm

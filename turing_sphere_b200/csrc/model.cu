@@ -99,7 +99,7 @@ const std::map<std::string, std::string> kCudaFn = {
     {"exp", "expf"},    {"floor", "floorf"}, {"log", "logf"},   {"log2", "log2f"},
     {"max", "fmaxf"},   {"min", "fminf"},    {"round", "roundf"}, {"sign", "ts_sign"},
     {"sin", "sinf"},    {"sinh", "sinhf"},   {"sqrt", "sqrtf"}, {"tan", "tanf"},
-    {"tanh", "tanhf"}};
+    {"tanh", "tanhf"}, {"__ge_sel", "ts_ge_sel"}};
 
 struct Emitter {
   const tsm::Function &f;
@@ -156,6 +156,31 @@ std::vector<int> stmt_inputs(const tsm::Stmt &s) {
 
 }  // namespace
 
+// The step's adjoint: per statement of `step` a generated forward ("tape")
+// and reverse kernel (element-wise statements) or the transform adjoints
+// (synth / analys); every value of the step has a tape buffer and, unless it
+// is a constant (lam, noise), a cotangent buffer, [instance][count].
+struct AdjStmt {
+  int stmt = -1;
+  std::string fwd_name, rev_name;
+  cudaKernel_t fwd = nullptr, rev = nullptr;
+  std::vector<int> in;       // value inputs, in the order of TsAdjIO::in
+  std::vector<int> dvars;    // inputs that receive cotangents (TsAdjIO::gin)
+};
+struct Adjoint {
+  bool ready = false;
+  cudaLibrary_t lib = nullptr;
+  std::vector<AdjStmt> st;
+  std::vector<float *> val, bar;  // per value of the step function
+  std::vector<long> count;        // floats per instance
+  std::vector<long> stride;       // per-instance stride of val (0 = shared)
+  std::vector<bool> constant;     // no cotangent (lam, noise)
+  std::vector<int> state_in, state_out;
+  double *pbar = nullptr;         // [instance][nparams]
+  float *tmp = nullptr;           // transform-adjoint output
+  std::vector<float *> owned;
+};
+
 struct ts_model_s {
   ts_ctx ctx = nullptr;
   ts_plan plan = nullptr;
@@ -180,6 +205,7 @@ struct ts_model_s {
   std::vector<StepGraph> graphs;
   bool use_graphs = true;
   int eager_left = 2;  // steps run eagerly first: every lazily grown buffer exists after them
+  Adjoint adj;
 };
 
 namespace {
@@ -590,13 +616,26 @@ std::string stage_title(const Stage &s) { return s.label; }
 
 // NVRTC: the generated stages plus the kernel headers -> an sm_100a cubin,
 // and the lowered name of every template instantiation.
+std::vector<char> nvrtc_cubin(const std::string &code, const std::vector<std::string> &exprs,
+                              std::map<std::string, std::string> &lowered);
+
 std::vector<char> build_cubin(ts_model m, std::map<std::string, std::string> &lowered) {
   std::ostringstream src;
   src << "#include \"ts_common.cuh\"\n#include \"fft2.cuh\"\n#include \"fourier.cuh\"\n#include \"leg_f32.cuh\"\n"
       << "#include \"leg_tc.cuh\"\n";
   for (auto &P : m->prog)
     for (auto &s : P.stages) src << stage_source(s);
-  const std::string code = src.str();
+  std::vector<std::string> exprs;
+  for (auto &P : m->prog)
+    for (auto &s : P.stages)
+      if (!s.expr.empty() && s.expr.find('<') != std::string::npos) exprs.push_back(s.expr);
+  return nvrtc_cubin(src.str(), exprs, lowered);
+}
+
+// NVRTC: source (with the embedded kernel headers) -> an sm_100a cubin, and
+// the lowered name of every template-instantiation expression
+std::vector<char> nvrtc_cubin(const std::string &code, const std::vector<std::string> &exprs,
+                              std::map<std::string, std::string> &lowered) {
   nvrtcProgram prog;
   auto nv = [&](nvrtcResult r, const char *what) {
     if (r != NVRTC_SUCCESS)
@@ -604,13 +643,7 @@ std::vector<char> build_cubin(ts_model m, std::map<std::string, std::string> &lo
   };
   nv(nvrtcCreateProgram(&prog, code.c_str(), "model.cu", ts_src_count, ts_src_texts, ts_src_names),
      "nvrtcCreateProgram");
-  std::vector<std::string> exprs;
-  for (auto &P : m->prog)
-    for (auto &s : P.stages)
-      if (!s.expr.empty() && s.expr.find('<') != std::string::npos) {
-        exprs.push_back(s.expr);
-        nv(nvrtcAddNameExpression(prog, s.expr.c_str()), "nvrtcAddNameExpression");
-      }
+  for (auto &e : exprs) nv(nvrtcAddNameExpression(prog, e.c_str()), "nvrtcAddNameExpression");
   const char *opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-lineinfo",
                         "--device-as-default-execution-space"};
   const nvrtcResult rc = nvrtcCompileProgram(prog, 4, opts);
@@ -851,7 +884,271 @@ void run_steps_graphed(ts_model m, int nsteps) {
   TS_CUDA(cudaGraphLaunch(exec, st));
 }
 
+float *dalloc(long n);
+
+// ------------------------------------------------------------------- adjoint
+//
+// Reverse mode over the step function, statement by statement:
+//   out = e(x..., params):  xbar += de/dx * outbar,  pbar += sum de/dp * outbar
+//   out = synth(x):         xbar += S^T outbar = c * analys(outbar / w)
+//   out = analys(x):        xbar += A^T outbar = w * synth(outbar / c)
+// with the derivatives of e generated symbolically (mdiff.cpp).  The
+// forward values come from an unfused replay of the step (the tape);
+// forward_backward checkpoints the state every K steps and replays each
+// segment from its checkpoint.
+
+std::string adj_source(ts_model m) {
+  Adjoint &A = m->adj;
+  const tsm::Function &f = m->prog[1].fn;
+  const int nprm = std::max<int>((int)m->params.size(), 1);
+  std::ostringstream src;
+  src << "#include \"ts_common.cuh\"\n";
+  for (auto &as : A.st) {
+    const tsm::Stmt &s = f.body[as.stmt];
+    if (s.kind != tsm::Stmt::Elementwise) continue;
+    Emitter em{f, {}};
+    for (size_t k = 0; k < as.in.size(); k++) em.name[as.in[k]] = "x" + std::to_string(k);
+    std::ostringstream loads;
+    for (size_t k = 0; k < as.in.size(); k++)
+      loads << "    const float x" << k << " = io.in[" << k << "][inst * io.in_stride[" << k
+            << "] + idx];\n";
+    // forward
+    src << "extern \"C\" __global__ void __launch_bounds__(256) " << as.fwd_name
+        << "(TsAdjIO io) {\n  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+        << "  if (idx >= io.n) return;\n  const long inst = blockIdx.y;\n"
+        << "  const float *prm = io.prm + inst * io.nprm;\n  (void)prm;\n"
+        << em.scalars() << loads.str()
+        << "  io.out[inst * io.out_stride + idx] = " << em.e(s.expr) << ";\n}\n";
+    // reverse
+    std::vector<std::pair<int, std::string>> dp;  // parameter slot, derivative
+    for (int j = 0; j < (int)m->params.size(); j++) {
+      const tsm::ExprP d = tsm::differentiate(f, s.expr, tsm::Wrt{tsm::Wrt::Param, j});
+      if (!tsm::is_zero(d)) dp.push_back({j, em.e(d)});
+    }
+    src << "extern \"C\" __global__ void __launch_bounds__(256) " << as.rev_name
+        << "(TsAdjIO io) {\n  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;\n"
+        << "  const bool live = idx < io.n;\n  const long inst = blockIdx.y;\n"
+        << "  const float *prm = io.prm + inst * io.nprm;\n  (void)prm;\n" << em.scalars();
+    if (!dp.empty()) src << "  float gp[" << dp.size() << "] = {};\n";
+    src << "  if (live) {\n" << loads.str()
+        << "    const float gb = io.gout[inst * io.gout_stride + idx];\n";
+    for (size_t k = 0; k < as.dvars.size(); k++) {
+      const tsm::ExprP d = tsm::differentiate(f, s.expr, tsm::Wrt{tsm::Wrt::Var, as.dvars[k]});
+      src << "    io.gin[" << k << "][inst * io.gin_stride[" << k << "] + idx] += (" << em.e(d)
+          << ") * gb;\n";
+    }
+    for (size_t j = 0; j < dp.size(); j++) src << "    gp[" << j << "] = (" << dp[j].second << ") * gb;\n";
+    src << "  }\n";
+    if (!dp.empty()) {
+      src << "  __shared__ float red[8];\n"
+          << "  for (int j = 0; j < " << dp.size() << "; j++) {\n"
+          << "    float v = gp[j];\n"
+          << "    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);\n"
+          << "    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;\n"
+          << "    __syncthreads();\n"
+          << "    if (threadIdx.x == 0) {\n"
+          << "      float t = 0.f;\n"
+          << "      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];\n"
+          << "      const int slot[" << dp.size() << "] = {";
+      for (size_t j = 0; j < dp.size(); j++) src << (j ? ", " : "") << dp[j].first;
+      src << "};\n"
+          << "      atomicAdd(io.pbar + inst * " << nprm << " + slot[j], (double)t);\n"
+          << "    }\n    __syncthreads();\n  }\n";
+    }
+    src << "}\n";
+  }
+  return src.str();
+}
+
+float *adj_alloc(Adjoint &A, long n) {
+  float *q = dalloc(std::max<long>(n, 1));
+  A.owned.push_back(q);
+  return q;
+}
+
+// the adjoint's statement list and value classes (no device work)
+void adj_structure(ts_model m) {
+  Adjoint &A = m->adj;
+  const tsm::Function &f = m->prog[1].fn;
+  ts_plan p = m->plan;
+  const int nv = (int)f.vars.size();
+  const long npts = (long)p->nlat * p->nphi, nspec = 2 * p->nlm;
+  A.st.clear();
+  A.val.assign(nv, nullptr);
+  A.bar.assign(nv, nullptr);
+  A.count.assign(nv, 0);
+  A.stride.assign(nv, 0);
+  A.constant.assign(nv, false);
+  for (int v = 0; v < nv; v++) {
+    const Dom d = f.vars[v].dom;
+    if (d == Dom::Scalar) continue;
+    A.count[v] = d == Dom::Grid ? npts : nspec;
+    A.stride[v] = A.count[v];
+    const int pi = f.vars[v].param_index;
+    if (pi >= 0) {
+      const std::string &name = f.param_names[pi];
+      A.constant[v] = std::find(m->state.begin(), m->state.end(), name) == m->state.end();
+    }
+  }
+  A.state_in.assign(m->state.size(), -1);
+  A.state_out.assign(m->state.size(), -1);
+  for (size_t s = 0; s < m->state.size(); s++) {
+    for (size_t i = 0; i < f.param_names.size(); i++)
+      if (f.param_names[i] == m->state[s]) A.state_in[s] = f.param_vars[i];
+    if (s < f.output_vars.size()) A.state_out[s] = f.output_vars[s];
+    TS_REQUIRE(A.state_in[s] >= 0 && A.state_out[s] >= 0, TS_ERR_UNSUPPORTED,
+               "adjoint: step must take and return every state");
+  }
+  int tag = 0;
+  for (size_t i = 0; i < f.body.size(); i++) {
+    const tsm::Stmt &s = f.body[i];
+    AdjStmt as;
+    as.stmt = (int)i;
+    if (s.kind == tsm::Stmt::Elementwise) {
+      as.in = stmt_inputs(s);
+      TS_REQUIRE(as.in.size() <= TS_MAXIO, TS_ERR_UNSUPPORTED,
+                 "adjoint: more than 8 values in one statement");
+      for (int v : as.in)
+        if (!A.constant[v]) as.dvars.push_back(v);
+      as.fwd_name = "ts_adj_f" + std::to_string(tag);
+      as.rev_name = "ts_adj_r" + std::to_string(tag++);
+    }
+    A.st.push_back(as);
+  }
+}
+
+// build (once) the adjoint program of the step function: buffers, kernels
+void adj_prepare(ts_model m) {
+  Adjoint &A = m->adj;
+  if (A.ready) return;
+  adj_structure(m);
+  const tsm::Function &f = m->prog[1].fn;
+  const int B = m->batch, nv = (int)f.vars.size();
+  for (int v = 0; v < nv; v++) {
+    if (A.count[v] == 0) continue;
+    const int pi = f.vars[v].param_index;
+    if (A.constant[v]) {  // lam, noise: host-owned
+      HostBuf &h = m->host.at(f.param_names[pi]);
+      A.val[v] = h.cur;
+      A.stride[v] = h.shared ? 0 : h.count;
+      continue;
+    }
+    if (pi < 0) A.val[v] = adj_alloc(A, A.count[v] * B);  // states: bound per replayed step
+    A.bar[v] = adj_alloc(A, A.count[v] * B);
+  }
+  const long npts = (long)m->plan->nlat * m->plan->nphi, nspec = 2 * m->plan->nlm;
+  A.tmp = adj_alloc(A, std::max(npts, nspec) * B);
+  TS_CUDA(cudaMalloc(&A.pbar, sizeof(double) * std::max<size_t>(m->params.size(), 1) * B));
+  std::map<std::string, std::string> lowered;
+  const std::vector<char> cubin = nvrtc_cubin(adj_source(m), {}, lowered);
+  TS_CUDA(cudaLibraryLoadData(&A.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+  for (auto &as : A.st)
+    if (!as.fwd_name.empty()) {
+      TS_CUDA(cudaLibraryGetKernel(&as.fwd, A.lib, as.fwd_name.c_str()));
+      TS_CUDA(cudaLibraryGetKernel(&as.rev, A.lib, as.rev_name.c_str()));
+    }
+  A.ready = true;
+}
+
+void adj_free(Adjoint &A) {
+  for (float *q : A.owned) cudaFree(q);
+  A.owned.clear();
+  if (A.pbar) cudaFree(A.pbar);
+  A.pbar = nullptr;
+  if (A.lib) cudaLibraryUnload(A.lib);
+  A.lib = nullptr;
+  A.ready = false;
+}
+
+TsAdjIO adj_io(ts_model m, const AdjStmt &as) {
+  Adjoint &A = m->adj;
+  const tsm::Stmt &s = m->prog[1].fn.body[as.stmt];
+  TsAdjIO io;
+  memset(&io, 0, sizeof io);
+  for (size_t k = 0; k < as.in.size(); k++) {
+    io.in[k] = A.val[as.in[k]];
+    io.in_stride[k] = A.stride[as.in[k]];
+  }
+  io.out = A.val[s.out];
+  io.out_stride = A.stride[s.out];
+  io.gout = A.bar[s.out];
+  io.gout_stride = A.count[s.out];
+  for (size_t k = 0; k < as.dvars.size(); k++) {
+    io.gin[k] = A.bar[as.dvars[k]];
+    io.gin_stride[k] = A.count[as.dvars[k]];
+  }
+  io.prm = m->d_prm;
+  io.nprm = std::max<int>((int)m->params.size(), 1);
+  io.pbar = A.pbar;
+  io.n = A.count[s.out];
+  return io;
+}
+
+__global__ void ts_k_axpy(float *y, const float *x, long n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+
+void axpy(float *y, const float *x, long n, cudaStream_t st) {
+  const int blocks = (int)std::min<long>((n + 255) / 256, 148L * 8);
+  ts_k_axpy<<<blocks, 256, 0, st>>>(y, x, n);
+  TS_CUDA(cudaGetLastError());
+}
+
+// the step's values from the states at `states[s]` ([instance][2 nlm] each)
+void adj_tape(ts_model m, const std::vector<const float *> &states, cudaStream_t st) {
+  Adjoint &A = m->adj;
+  const tsm::Function &f = m->prog[1].fn;
+  const int B = m->batch;
+  for (size_t s = 0; s < states.size(); s++) A.val[A.state_in[s]] = const_cast<float *>(states[s]);
+  for (auto &as : A.st) {
+    const tsm::Stmt &s = f.body[as.stmt];
+    if (s.kind == tsm::Stmt::Elementwise) {
+      TsAdjIO io = adj_io(m, as);
+      void *args[] = {&io};
+      dim3 grid((unsigned)((io.n + 255) / 256), B);
+      TS_CUDA(cudaLaunchKernel((const void *)as.fwd, grid, dim3(256), args, 0, st));
+    } else if (s.kind == tsm::Stmt::Synth) {
+      ts_synth_dev(m->plan, A.val[s.arg], A.val[s.out], B, st);
+    } else {
+      ts_analys_dev(m->plan, A.val[s.arg], A.val[s.out], B, st);
+    }
+  }
+}
+
+// one reverse step: lam[s] (cotangent of the step's output state s) in,
+// cotangent of its input state s out (in place); parameter gradients add up
+void adj_reverse(ts_model m, const std::vector<float *> &lam, cudaStream_t st) {
+  Adjoint &A = m->adj;
+  const tsm::Function &f = m->prog[1].fn;
+  const int B = m->batch;
+  for (size_t v = 0; v < A.bar.size(); v++)
+    if (A.bar[v]) TS_CUDA(cudaMemsetAsync(A.bar[v], 0, sizeof(float) * A.count[v] * B, st));
+  for (size_t s = 0; s < lam.size(); s++) axpy(A.bar[A.state_out[s]], lam[s], A.count[A.state_out[s]] * B, st);
+  for (auto it = A.st.rbegin(); it != A.st.rend(); ++it) {
+    const tsm::Stmt &s = f.body[it->stmt];
+    if (s.kind == tsm::Stmt::Elementwise) {
+      if (it->dvars.empty() && m->params.empty()) continue;
+      TsAdjIO io = adj_io(m, *it);
+      void *args[] = {&io};
+      dim3 grid((unsigned)((io.n + 255) / 256), B);
+      TS_CUDA(cudaLaunchKernel((const void *)it->rev, grid, dim3(256), args, 0, st));
+    } else if (!A.constant[s.arg]) {
+      if (s.kind == tsm::Stmt::Synth)
+        ts_synth_adjoint(m->plan, A.bar[s.out], A.tmp, B, st);
+      else
+        ts_analys_adjoint(m->plan, A.bar[s.out], A.tmp, B, st);
+      axpy(A.bar[s.arg], A.tmp, A.count[s.arg] * B, st);
+    }
+  }
+  for (size_t s = 0; s < lam.size(); s++)
+    TS_CUDA(cudaMemcpyAsync(lam[s], A.bar[A.state_in[s]], sizeof(float) * A.count[A.state_in[s]] * B,
+                            cudaMemcpyDeviceToDevice, st));
+}
+
 void free_model(ts_model m) {
+  adj_free(m->adj);
   drop_graphs(m);
   for (auto &kv : m->host) {
     if (kv.second.cur) cudaFree(kv.second.cur);
@@ -868,6 +1165,17 @@ void free_model(ts_model m) {
   m->wimg.release();
   if (m->lib) cudaLibraryUnload(m->lib);
 }
+
+// device memory released at scope exit
+struct DevMem {
+  void *p = nullptr;
+  explicit DevMem(size_t bytes) { TS_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16))); }
+  ~DevMem() {
+    if (p) cudaFree(p);
+  }
+  DevMem(const DevMem &) = delete;
+  DevMem &operator=(const DevMem &) = delete;
+};
 
 float *dalloc(long n) {
   float *p = nullptr;
@@ -1123,12 +1431,12 @@ int ts_model_init(ts_model m, const float *noise, long n) {
   TSM_END
 }
 
-int ts_model_step(ts_model m, int nsteps) {
-  TSM_BEGIN(m)
-  TS_REQUIRE(nsteps >= 0, TS_ERR_INVALID, "nsteps must be >= 0");
+namespace {
+// nsteps steps: eager warm-up steps, then captured graphs
+void advance(ts_model m, int nsteps) {
   int done = 0;
   for (; done < nsteps && (m->eager_left > 0 || !graphs_usable(m)); done++) {
-    run_program(m, m->prog[1], ctx->stream);
+    run_program(m, m->prog[1], m->ctx->stream);
     if (m->eager_left > 0) m->eager_left--;
   }
   while (nsteps - done >= 2) {
@@ -1137,6 +1445,67 @@ int ts_model_step(ts_model m, int nsteps) {
   }
   if (done < nsteps) run_steps_graphed(m, 1);
   if (nsteps > 0) m->last_ran = 1;
+}
+}  // namespace
+
+int ts_model_step(ts_model m, int nsteps) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(nsteps >= 0, TS_ERR_INVALID, "nsteps must be >= 0");
+  advance(m, nsteps);
+  TSM_END
+}
+
+int ts_model_forward_backward(ts_model m, int nsteps, int every, const float *final_bar,
+                              float *init_bar, double *param_bar) {
+  TSM_BEGIN(m)
+  TS_REQUIRE(nsteps >= 1 && every >= 1, TS_ERR_INVALID, "nsteps and every must be >= 1");
+  TS_REQUIRE(final_bar && init_bar, TS_ERR_INVALID, "null argument");
+  adj_prepare(m);
+  Adjoint &A = m->adj;
+  cudaStream_t st = ctx->stream;
+  const int B = m->batch, ns = (int)m->state.size();
+  const long sz = 2 * m->plan->nlm * (long)B;  // floats of one state, all instances
+  const int nseg = (nsteps + every - 1) / every;
+  // checkpoints [segment][state], segment states [step][state], cotangents [state]
+  DevMem ck(sizeof(float) * sz * ns * nseg), seg(sizeof(float) * sz * ns * every),
+      lamb(sizeof(float) * sz * ns);
+  float *pck = (float *)ck.p, *pseg = (float *)seg.p, *plam = (float *)lamb.p;
+  for (int i = 0; i < nsteps; i += every) {
+    for (int s = 0; s < ns; s++)
+      TS_CUDA(cudaMemcpyAsync(pck + ((long)(i / every) * ns + s) * sz, m->host.at(m->state[s]).cur,
+                              sizeof(float) * sz, cudaMemcpyDeviceToDevice, st));
+    advance(m, std::min(every, nsteps - i));
+  }
+  TS_CUDA(cudaMemcpyAsync(plam, final_bar, sizeof(float) * sz * ns, cudaMemcpyHostToDevice, st));
+  TS_CUDA(cudaMemsetAsync(A.pbar, 0, sizeof(double) * std::max<size_t>(m->params.size(), 1) * B, st));
+  std::vector<float *> lam(ns);
+  for (int s = 0; s < ns; s++) lam[s] = plam + (long)s * sz;
+  for (int g = nseg - 1; g >= 0; g--) {
+    const int len = std::min(every, nsteps - g * every);
+    TS_CUDA(cudaMemcpyAsync(pseg, pck + (long)g * ns * sz, sizeof(float) * sz * ns,
+                            cudaMemcpyDeviceToDevice, st));
+    auto states = [&](int j) {
+      std::vector<const float *> v(ns);
+      for (int s = 0; s < ns; s++) v[s] = pseg + ((long)j * ns + s) * sz;
+      return v;
+    };
+    for (int j = 1; j < len; j++) {  // replay the segment: the state before every step
+      adj_tape(m, states(j - 1), st);
+      for (int s = 0; s < ns; s++)
+        TS_CUDA(cudaMemcpyAsync(pseg + ((long)j * ns + s) * sz, A.val[A.state_out[s]],
+                                sizeof(float) * sz, cudaMemcpyDeviceToDevice, st));
+    }
+    for (int j = len - 1; j >= 0; j--) {
+      adj_tape(m, states(j), st);
+      adj_reverse(m, lam, st);
+    }
+  }
+  TS_CUDA(cudaMemcpyAsync(init_bar, plam, sizeof(float) * sz * ns, cudaMemcpyDeviceToHost, st));
+  if (param_bar && !m->params.empty())
+    TS_CUDA(cudaMemcpyAsync(param_bar, A.pbar, sizeof(double) * m->params.size() * B,
+                            cudaMemcpyDeviceToHost, st));
+  TS_CUDA(cudaStreamSynchronize(st));
+  TS_CUDA(cudaGetLastError());
   TSM_END
 }
 
@@ -1291,11 +1660,17 @@ int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
     finish_shapes(&mod);
     std::map<std::string, std::string> lowered;
     build_cubin(&mod, lowered);
+    std::string adj_code;
+    if (flags & TS_CHECK_ADJOINT) {
+      adj_structure(&mod);
+      adj_code = adj_source(&mod);
+      nvrtc_cubin(adj_code, {}, lowered);
+    }
     if (describe && cap && (flags & TS_CHECK_SOURCE)) {
       std::string code;
       for (auto &P : mod.prog)
         for (auto &st : P.stages) code += stage_source(st);
-      snprintf(describe, cap, "%s", code.c_str());
+      snprintf(describe, cap, "%s%s", code.c_str(), adj_code.c_str());
     } else if (describe && cap) {
       snprintf(describe, cap, "%s====\n%s", describe_program(mod.prog[0]).c_str(),
                describe_program(mod.prog[1]).c_str());

@@ -73,14 +73,20 @@ struct ts_plan_s {
   float2 *d_ab = nullptr, *d_tw = nullptr;
   TsLegTab leg{};
   TsFftTab fft{};
-  // scratch: fm intermediate, host-call staging
-  ts_dbuf fm, stage_q, stage_s;
+  // scratch: fm intermediate, host-call staging, adjoint scalings
+  ts_dbuf fm, stage_q, stage_s, adj_grid, adj_spec;
   // tensor-core tables (precision != FP32)
   void *tc = nullptr;
   // kernel shapes: 0 = default (or TS_TC_NL / TS_TC_LTL); set by the autotuner
   int tune_nl = 0, tune_ltl = 0, fft_rows = 0;
   bool tuned = false;
 };
+
+// whole transforms on device buffers (capi.cu) and their adjoints (adjoint.cu)
+void ts_synth_dev(ts_plan p, const float *qlm, float *spat, int batch, cudaStream_t s);
+void ts_analys_dev(ts_plan p, const float *spat, float *qlm, int batch, cudaStream_t s);
+void ts_synth_adjoint(ts_plan p, const float *gbar, float *qbar, int nf, cudaStream_t s);
+void ts_analys_adjoint(ts_plan p, const float *qbar, float *gbar, int nf, cudaStream_t s);
 
 // autotune.cu: time the candidate kernel shapes of a plan, keep the fastest
 void ts_autotune(ts_plan p);

@@ -115,6 +115,36 @@ class GpuModel:
     def step(self, steps: int = 1) -> None:
         self._check(_lib.lib().ts_model_step(self.handle, steps))
 
+    def forwardBackward(self, nsteps: int, every: int, finalBar):
+        """The adjoint's forward/backward pair (no reference counterpart; the
+        autograd.Function of this path): advance ``nsteps`` steps keeping a
+        state checkpoint every ``every`` steps, then run the hand-written
+        adjoint backwards.  ``finalBar``: dL/d(final state), a dict state ->
+        (instances, 2 nlm) array (missing states: zero).  Returns
+        (dL/d(initial state) as such a dict, dL/d(params) as an
+        (instances, nparams) float64 array in ``paramNames`` order)."""
+        ns, B, n2 = len(self.state), self.batch, 2 * self.nlm
+        fb = np.zeros((ns, B, n2), dtype=np.float32)
+        for i, s in enumerate(self.state):
+            if s in finalBar:
+                fb[i] = np.asarray(finalBar[s], dtype=np.float32).reshape(B, n2)
+        ib = np.zeros_like(fb)
+        pb = np.zeros((B, max(len(self.paramNames), 1)), dtype=np.float64)
+        self._check(_lib.lib().ts_model_forward_backward(
+            self.handle, nsteps, every, _lib.fptr(fb), _lib.fptr(ib), _lib.dptr(pb)))
+        return {s: ib[i] for i, s in enumerate(self.state)}, pb[:, :len(self.paramNames)]
+
+    def lossGradient(self, nsteps: int, every: int, finalBarOf):
+        """Gradient of a loss of the final state: ``finalBarOf(final)`` maps
+        the final states (dict state -> (instances, 2 nlm) array) to
+        dL/d(final state); the model ends at the final state, as after
+        ``step(nsteps)``.  Returns what forwardBackward returns."""
+        self.snapshotState()
+        self.step(nsteps)
+        final = {s: self.read(s).reshape(self.batch, -1) for s in self.state}
+        self.restoreState()
+        return self.forwardBackward(nsteps, every, finalBarOf(final))
+
     def setGraphs(self, enable: bool) -> None:
         """Run steps as captured CUDA graphs (default) or launch them eagerly."""
         self._check(_lib.lib().ts_model_set_graphs(self.handle, 1 if enable else 0))

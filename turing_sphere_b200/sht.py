@@ -145,6 +145,18 @@ class ShtPlan:
         _lib.check(_lib.lib().ts_sht_analys_dev(self.handle, spat_ptr, qlm_ptr, batch, stream),
                    self.device.handle)
 
+    def synth_adjoint_dev(self, gbar_ptr: int, qbar_ptr: int, batch: int = 1,
+                          stream: int | None = None):
+        """qbar = S^T gbar: the transpose of synth_dev (grid -> spectral)."""
+        _lib.check(_lib.lib().ts_sht_synth_adjoint_dev(self.handle, gbar_ptr, qbar_ptr, batch,
+                                                       stream), self.device.handle)
+
+    def analys_adjoint_dev(self, qbar_ptr: int, gbar_ptr: int, batch: int = 1,
+                           stream: int | None = None):
+        """gbar = A^T qbar: the transpose of analys_dev (spectral -> grid)."""
+        _lib.check(_lib.lib().ts_sht_analys_adjoint_dev(self.handle, qbar_ptr, gbar_ptr, batch,
+                                                        stream), self.device.handle)
+
     def wimageBytes(self, batch: int) -> int:
         """Bytes of the tensor-core analysis operand image for `batch` fields
         (0 on an FP32 plan)."""
