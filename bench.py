@@ -384,6 +384,108 @@ def time_imex_config1(dev, stream, precision, K=2000, graphs=True):
     return K / (ms / 1e3)
 
 
+def time_config3(dev, stream, K=200):
+    """Brusselator parameter sweep: 256 instances with (A, B) spread over the
+    Turing-unstable band, lmax 127 on 192 x 384, tensor-core plan, steps as
+    captured graphs.  Returns instance-steps/s."""
+    import torch
+    from turing_sphere_b200 import (GpuModel, ShtConfig, ShtPlan, defaultParams, mModelByKey,
+                                    seededNoise)
+    model = mModelByKey("brusselator")
+    base = defaultParams(model)
+    ni, npts = 256, 192 * 384
+    rng = np.random.default_rng(3)
+    sweep = []
+    for _ in range(ni):
+        a = rng.uniform(2.5, 3.5)
+        lo = (1 + a * math.sqrt(base["D1"] / base["D2"])) ** 2
+        sweep.append(dict(base, A=a, B=rng.uniform(lo, 1 + a * a)))
+    plan = ShtPlan.create(dev, ShtConfig(127, 127, 192, 384), {"precision": "tf32x3",
+                                                               "autotune": True})
+    gpu = GpuModel.create(dev, plan, model.source, [q.key for q in model.params], model.state,
+                          model.species, ni)
+    gpu.setParams(sweep)
+    gpu.init(np.concatenate([seededNoise(npts, model.seedAmp, 1 + k) for k in range(ni)]))
+    gpu.step(5)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    gpu.step(K)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    finite = bool(np.isfinite(gpu.read("U")).all())
+    gpu.destroy()
+    plan.destroy()
+    return {"workload": "Brusselator sweep, 256 instances, lmax 127, 192x384, tf32x3, "
+                        f"{K} steps as captured step graphs",
+            "instance_steps_per_s": ni * K / (ms / 1e3), "finite": finite}
+
+
+def time_ragged(dev, stream, K=100):
+    """Config 3's ragged variant: 64 Brusselator instances at each of lmax
+    63/127/255 (96x192, 192x384, 384x768 grids, one plan and model each),
+    advanced as one model group (one captured graph per step, the three
+    models on concurrent branches).  Returns instance-steps/s over all 192."""
+    import torch
+    from turing_sphere_b200 import (GpuModel, ModelGroup, ShtConfig, ShtPlan, defaultParams,
+                                    mModelByKey, seededNoise)
+    model = mModelByKey("brusselator")
+    p = defaultParams(model)
+    parts = []
+    for lmax, nlat in ((63, 96), (127, 192), (255, 384)):
+        plan = ShtPlan.create(dev, ShtConfig(lmax, lmax, nlat, 2 * nlat),
+                              {"precision": "tf32x3", "autotune": True})
+        gpu = GpuModel.create(dev, plan, model.source, [q.key for q in model.params],
+                              model.state, model.species, 64)
+        gpu.setParams(p)
+        gpu.init(np.concatenate([seededNoise(nlat * 2 * nlat, model.seedAmp, 1 + k)
+                                 for k in range(64)]))
+        parts.append((plan, gpu))
+    group = ModelGroup([g for _, g in parts])
+    group.step(6)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    group.step(K)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    group.destroy()
+    for plan, gpu in parts:
+        gpu.destroy()
+        plan.destroy()
+    return {"workload": "Brusselator, 64 instances at each of lmax 63/127/255, one model "
+                        f"group, {K} steps as captured group graphs",
+            "instance_steps_per_s": 192 * K / (ms / 1e3)}
+
+
+def time_adjoint(dev, key, lmax, nlat, nphi, ni, nsteps, every):
+    """Forward + adjoint (ts_model_forward_backward) of `key` with `ni`
+    instances: seconds for `nsteps` steps with checkpoints every `every`."""
+    from turing_sphere_b200 import (GpuModel, ShtConfig, ShtPlan, defaultParams, mModelByKey,
+                                    seededNoise)
+    model = mModelByKey(key)
+    plan = ShtPlan.create(dev, ShtConfig(lmax, lmax, nlat, nphi), {"precision": "tf32x3",
+                                                                   "autotune": True})
+    gpu = GpuModel.create(dev, plan, model.source, [q.key for q in model.params], model.state,
+                          model.species, ni)
+    gpu.setParams(defaultParams(model))
+    gpu.init(np.concatenate([seededNoise(nlat * nphi, model.seedAmp, 1 + k) for k in range(ni)]))
+    rng = np.random.default_rng(1)
+    bar = {s: rng.standard_normal((ni, 2 * plan.nlm)).astype(np.float32) for s in model.state}
+    gpu.forwardBackward(every, every, bar)  # compiles the adjoint, warms up
+    t0 = time.perf_counter()
+    _, pbar = gpu.forwardBackward(nsteps, every, bar)
+    dt = time.perf_counter() - t0
+    ok = bool(np.isfinite(pbar).all())
+    gpu.destroy()
+    plan.destroy()
+    return dt, ok
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -486,6 +588,10 @@ def main():
     imex_fp_ms, _, ok_fp = time_imex(dev, plain, ni, max(10, args.imex_steps // 4), 3, stream)
     c1_fp32 = time_imex_config1(dev, stream, "fp32")
     c1_tc = time_imex_config1(dev, stream, "tf32x3")
+    c3 = time_config3(dev, stream)
+    c3["ragged"] = time_ragged(dev, stream)
+    a4_s, a4_ok = time_adjoint(dev, "allencahn", 255, 384, 768, 1, 256, 32)
+    a5_s, a5_ok = time_adjoint(dev, "schnakenberg", 511, 768, 1536, 64, 64, 32)
 
     if rank == 0:
         hbm, bf16, src = measured_peaks()
@@ -544,6 +650,17 @@ def main():
                      "config1": {"workload": "1 Schnakenberg instance, lmax 63, 96x192, "
                                              "2000 steps as captured step graphs",
                                  "fp32_steps_per_s": c1_fp32, "tc_steps_per_s": c1_tc}},
+            "config3": c3,
+            "adjoint": {
+                "config4": {"workload": "Allen-Cahn, 1 instance, lmax 255, 384x768, tf32x3, "
+                                        "256 steps forward + adjoint, checkpoints every 32",
+                            "steps_per_s": 256 / a4_s, "finite": a4_ok},
+                "config5": {"workload": "Schnakenberg, 64 instances, lmax 511, 768x1536, "
+                                        "tf32x3, 64 steps forward + adjoint, checkpoints every 32, "
+                                        "gradients w.r.t. (a, b, D1, D2, dt) and the state",
+                            "instance_steps_per_s": 64 * 64 / a5_s, "finite": a5_ok},
+                "note": "wall-clock around ts_model_forward_backward (host round trips "
+                        "of the cotangents included)"},
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": sampler.summary(),

@@ -36,6 +36,7 @@ extern "C" {
 typedef struct ts_ctx_s *ts_ctx;
 typedef struct ts_plan_s *ts_plan;
 typedef struct ts_model_s *ts_model;
+typedef struct ts_group_s *ts_group;
 
 enum ts_status {
   TS_OK = 0,
@@ -233,6 +234,16 @@ int ts_model_step(ts_model model, int nsteps);
  * caller is capturing itself, or the legacy default stream, runs eagerly.
  * enable = 0 turns graphs off for this model (results are identical). */
 int ts_model_set_graphs(ts_model model, int enable);
+
+/* Model groups (no reference counterpart): ragged batches, e.g. instances
+ * at lmax 63/127/255 each compiled as one model on its own plan, advance
+ * together.  Each step runs every model's kernels on its own branch stream
+ * forked from the context stream; after two eager steps, steps are captured
+ * as one CUDA graph per state parity and replayed.  All models must share
+ * the context; a model in a group is stepped through the group only. */
+int ts_model_group_create(ts_model const *models, int n, ts_group *out);
+int ts_model_group_step(ts_group group, int nsteps);
+int ts_model_group_destroy(ts_group group);
 
 /* Forward/backward pair of the adjoint (no reference counterpart; the
  * autograd.Function of this path).  Advances the model nsteps steps from its

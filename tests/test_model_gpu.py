@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from turing_sphere_b200 import (GpuModel, ModelSession, ShtConfig, ShtPlan, defaultParams,
+from turing_sphere_b200 import (GpuModel, ModelGroup, ModelSession, ShtConfig, ShtPlan,
+                                defaultParams,
                                 gridForLmax, lmIndex, mModelByKey, mModels, nlmCalc, seededNoise)
 from turing_sphere_b200.registry import MModel, ParamSpec
 
@@ -251,6 +252,43 @@ def test_graph_steps_equal_eager_steps(device, precision):
         gpu.destroy()
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+def test_ragged_group_equals_separate_models(device):
+    """A ragged batch (Brusselator instances at lmax 15, 31 and 63 on their
+    own plans) stepped as one group (concurrent branches in one graph per
+    step) ends bit-identical to the same models stepped one by one."""
+    model = mModelByKey("brusselator")
+    base = defaultParams(model)
+    names = [q.key for q in model.params]
+    specs = [(15, 2), (31, 3), (63, 1)]
+
+    def build():
+        out = []
+        for lmax, ni in specs:
+            nlat, nphi = gridForLmax(lmax, model.pdeg)
+            sht = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi),
+                                 {"precision": "tf32x3"})
+            gpu = GpuModel.create(device, sht, model.source, names, list(model.state),
+                                  list(model.species), ni)
+            gpu.setParams([dict(base, A=base["A"] + 0.05 * k) for k in range(ni)])
+            gpu.init(np.concatenate([seededNoise(nlat * nphi, model.seedAmp, 3 + k)
+                                     for k in range(ni)]))
+            out.append((sht, gpu))
+        return out
+
+    grouped, single = build(), build()
+    group = ModelGroup([g for _, g in grouped])
+    for n in (1, 2, 3, 2):  # eager warm-up, then graphs at both parities
+        group.step(n)
+    for _, g in single:
+        g.step(8)
+    for (_, a), (_, b) in zip(grouped, single):
+        assert np.array_equal(a.read("U"), b.read("U"))
+        assert np.array_equal(a.read("V"), b.read("V"))
+    group.destroy()
+    for _, g in grouped + single:
+        g.destroy()
 
 
 def test_upload_and_read_errors(device):

@@ -111,6 +111,9 @@ SIGNATURES = {
     "ts_model_step": (i32, [vp, i32]),
     "ts_model_set_graphs": (i32, [vp, i32]),
     "ts_model_forward_backward": (i32, [vp, i32, i32, f32p, f32p, f64p]),
+    "ts_model_group_create": (i32, [C.POINTER(vp), i32, C.POINTER(vp)]),
+    "ts_model_group_step": (i32, [vp, i32]),
+    "ts_model_group_destroy": (i32, [vp]),
     "ts_model_read": (i32, [vp, cstr, f32p, i64]),
     "ts_model_value_ptr": (i32, [vp, cstr, C.POINTER(vp), C.POINTER(i64)]),
     "ts_model_snapshot": (i32, [vp]),

@@ -1455,6 +1455,166 @@ int ts_model_step(ts_model m, int nsteps) {
   TSM_END
 }
 
+// ------------------------------------------------------------ model groups
+//
+// Several models (ragged batches: instances at different lmax, each group
+// its own plan) advance together: every step runs each model's kernels on
+// its own branch stream, forked from and joined to the context stream by
+// events, captured into one CUDA graph per step pair and replayed, so the
+// models' kernels overlap on the GPU.
+
+struct ts_group_s {
+  std::vector<ts_model> models;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> done;
+  cudaEvent_t fork = nullptr;
+  struct G {
+    std::vector<float *> key;
+    int nsteps;
+    cudaGraphExec_t exec;
+  };
+  std::vector<G> graphs;
+  int eager_left = 2;
+  bool use_graphs = true;
+};
+
+namespace {
+
+std::vector<float *> group_key(ts_group g) {
+  std::vector<float *> k;
+  for (ts_model m : g->models) {
+    auto mk = state_key(m);
+    k.insert(k.end(), mk.begin(), mk.end());
+  }
+  return k;
+}
+
+// one step of every model, forked from / joined to the context stream
+void group_launch(ts_group g) {
+  cudaStream_t s0 = g->models[0]->ctx->stream;
+  TS_CUDA(cudaEventRecord(g->fork, s0));
+  for (size_t i = 0; i < g->models.size(); i++) {
+    TS_CUDA(cudaStreamWaitEvent(g->streams[i], g->fork, 0));
+    run_program(g->models[i], g->models[i]->prog[1], g->streams[i]);
+    TS_CUDA(cudaEventRecord(g->done[i], g->streams[i]));
+  }
+  for (size_t i = 0; i < g->models.size(); i++) TS_CUDA(cudaStreamWaitEvent(s0, g->done[i], 0));
+}
+
+void group_swap(ts_group g, int nsteps) {
+  for (ts_model m : g->models) swap_states(m, nsteps);
+}
+
+void group_steps(ts_group g, int nsteps) {
+  cudaStream_t s0 = g->models[0]->ctx->stream;
+  const std::vector<float *> key = group_key(g);
+  for (auto &x : g->graphs)
+    if (x.nsteps == nsteps && x.key == key) {
+      TS_CUDA(cudaGraphLaunch(x.exec, s0));
+      group_swap(g, nsteps);
+      return;
+    }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool ok = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    int ran = 0;
+    try {
+      for (; ran < nsteps; ran++) group_launch(g);
+    } catch (const ts_exc &) {
+      ok = false;
+    }
+    const bool ended = cudaStreamEndCapture(s0, &graph) == cudaSuccess;
+    ok = ok && ended && graph;
+    if (!ok) group_swap(g, ran);
+  }
+  if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok) {
+    (void)cudaGetLastError();
+    g->use_graphs = false;
+    for (int i = 0; i < nsteps; i++) group_launch(g);
+    return;
+  }
+  g->graphs.push_back({key, nsteps, exec});
+  TS_CUDA(cudaGraphLaunch(exec, s0));
+}
+
+}  // namespace
+
+int ts_model_group_create(ts_model const *models, int n, ts_group *out) {
+  ts_ctx ctx = (n > 0 && models && models[0]) ? models[0]->ctx : nullptr;
+  ts_group g = nullptr;
+  try {
+    TS_REQUIRE(ctx && out && n >= 1, TS_ERR_INVALID, "need at least one model and an output");
+    for (int i = 0; i < n; i++)
+      TS_REQUIRE(models[i] && models[i]->ctx == ctx, TS_ERR_INVALID,
+                 "group: every model must belong to the same context");
+    TS_CUDA(cudaSetDevice(ctx->device));
+    g = new ts_group_s();
+    g->models.assign(models, models + n);
+    TS_CUDA(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
+    for (int i = 0; i < n; i++) {
+      cudaStream_t st;
+      cudaEvent_t ev;
+      TS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      g->streams.push_back(st);
+      TS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      g->done.push_back(ev);
+    }
+    *out = g;
+    return TS_OK;
+  } catch (const ts_exc &e) {
+    if (g) ts_model_group_destroy(g);
+    ts_set_error(ctx, e.msg);
+    return e.code;
+  }
+}
+
+int ts_model_group_step(ts_group g, int nsteps) {
+  ts_ctx ctx = g && !g->models.empty() ? g->models[0]->ctx : nullptr;
+  try {
+    TS_REQUIRE(g != nullptr && nsteps >= 0, TS_ERR_INVALID, "bad group or step count");
+    TS_CUDA(cudaSetDevice(ctx->device));
+    const cudaStream_t s0 = ctx->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const bool capturable = g->use_graphs && s0 != nullptr && s0 != cudaStreamLegacy &&
+                            s0 != cudaStreamPerThread &&
+                            cudaStreamIsCapturing(s0, &cs) == cudaSuccess &&
+                            cs == cudaStreamCaptureStatusNone;
+    int done = 0;
+    for (; done < nsteps && (g->eager_left > 0 || !capturable); done++) {
+      group_launch(g);
+      if (g->eager_left > 0) g->eager_left--;
+    }
+    while (nsteps - done >= 2) {
+      group_steps(g, 2);
+      done += 2;
+    }
+    if (done < nsteps) group_steps(g, 1);
+    if (nsteps > 0)
+      for (ts_model m : g->models) m->last_ran = 1;
+    return TS_OK;
+  } catch (const ts_exc &e) {
+    ts_set_error(ctx, e.msg);
+    return e.code;
+  }
+}
+
+int ts_model_group_destroy(ts_group g) {
+  if (!g) return TS_ERR_INVALID;
+  if (!g->models.empty()) {
+    cudaSetDevice(g->models[0]->ctx->device);
+    cudaStreamSynchronize(g->models[0]->ctx->stream);
+  }
+  for (auto &x : g->graphs) cudaGraphExecDestroy(x.exec);
+  for (cudaStream_t st : g->streams) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : g->done) cudaEventDestroy(ev);
+  if (g->fork) cudaEventDestroy(g->fork);
+  delete g;
+  return TS_OK;
+}
+
 int ts_model_forward_backward(ts_model m, int nsteps, int every, const float *final_bar,
                               float *init_bar, double *param_bar) {
   TSM_BEGIN(m)

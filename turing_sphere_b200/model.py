@@ -322,3 +322,26 @@ class ModelSession:
         if self._displaySht:
             self._displaySht.destroy()
         self.sht.destroy()
+
+
+class ModelGroup:
+    """Ragged batches: several GpuModels (e.g. instances at different lmax,
+    each on its own plan) stepped together, every step one CUDA graph whose
+    branches run the models concurrently (ts_model_group_*)."""
+
+    def __init__(self, models):
+        self.models = list(models)
+        arr = (C.c_void_p * len(self.models))(*[m.handle.value if hasattr(m.handle, "value")
+                                                 else m.handle for m in self.models])
+        h = C.c_void_p()
+        dev = self.models[0].device
+        _lib.check(_lib.lib().ts_model_group_create(arr, len(self.models), C.byref(h)), dev.handle)
+        self.handle, self.device = h, dev
+
+    def step(self, n: int = 1) -> None:
+        _lib.check(_lib.lib().ts_model_group_step(self.handle, n), self.device.handle)
+
+    def destroy(self) -> None:
+        if self.handle:
+            _lib.lib().ts_model_group_destroy(self.handle)
+            self.handle = None
