@@ -119,6 +119,32 @@ class ClockSampler:
                 "reasons": names, "samples": len(self.samples)}
 
 
+PROFILE = os.path.join(ROOT, "profiles", "sht_pair_lmax255_b256_kernels.txt")
+STAGE_KERNELS = {"legSynth": ["ts_k_qimage", "ts_leg_synth_tc"], "fourSynth": ["ts_f2_synth"],
+                 "fourAnalysW": ["ts_f2_analys_w"], "legAnalysW": ["ts_leg_analys_tc"],
+                 "fourAnalys": ["ts_f2_analys<"], "legAnalys": ["ts_leg_analys"]}
+
+
+def profiled_traffic(stage):
+    """DRAM bytes (read + write) of one launch of the stage's kernels, from
+    the committed ncu summary of this workload, or None."""
+    if not os.path.exists(PROFILE):
+        return None
+    total, found = 0.0, False
+    with open(PROFILE) as fh:
+        for line in fh:
+            if not line.startswith("kernel ") or "dram_read_MB" not in line:
+                continue
+            name = line[len("kernel "):line.index(" time_us")]
+            if not any(name.startswith(k) for k in STAGE_KERNELS[stage]):
+                continue
+            f = line.split()
+            total += (float(f[f.index("dram_read_MB") + 1]) +
+                      float(f[f.index("dram_write_MB") + 1])) * 1e6
+            found = True
+    return total if found else None
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -623,6 +649,9 @@ def main():
                     "peak": hbm, "unit": "GB/s", "frac": alg_bytes / dur / 1e9 / hbm,
                     "traffic": None, "peak_source": f"{src} hbm_gbs (of measured)",
                     "algorithmic_bytes": alg_bytes}
+        roof["traffic"] = profiled_traffic(name)
+        roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                  "launch (profiles/sht_pair_lmax255_b256_kernels.txt)")
         roof["stage_ms"] = stage_ms
         cpu = cpu_baseline(lmax, nlat, nphi, budget_s=10.0, threads=0)
         line = {
