@@ -118,6 +118,14 @@ int ts_sht_plan_info(ts_plan plan, ts_plan_info *info);
  * the flag) if a tensor-core kernel of this plan gave up a bounded wait for its
  * MMAs since the last call; TS_OK otherwise. */
 int ts_sht_plan_status(ts_plan plan);
+/* Test hook for failure detection (no reference counterpart).  With
+ * stall_copies != 0 the tensor-core kernels' copy warp issues no copies, so
+ * every bounded wait of the kernel runs out after `wait_limit` polls (0 =
+ * the default limit): the kernel records the error, frees its tensor memory
+ * and returns, and ts_sht_plan_status reports TS_ERR_TIMEOUT once.  Nothing
+ * faults or hangs; stall_copies = 0 restores normal operation.
+ * TS_ERR_UNSUPPORTED on FP32 plans. */
+int ts_sht_plan_test_stall(ts_plan plan, int stall_copies, unsigned wait_limit);
 
 /* Nodes x_i = cos(theta_i) (decreasing) and Gauss weights w_i, f64, nlat each,
  * as computed on the GPU (ShtPlan.cosTheta / gaussWeights, sht.ts:120-125). */

@@ -125,3 +125,35 @@ def test_autotuned_plan_keeps_parity(device):
     assert again.shapes == sh
     default = tc_plan(device, lmax, nlat, nphi)
     assert not default.shapes["tuned"] and default.shapes["tc_lat_tile"] == 96
+
+
+def test_bounded_waits_time_out_and_the_plan_recovers(device):
+    """Failure detection without a GPU fault: with the copy warp stalled (the
+    plan's test hook) every bounded mbarrier wait of the tensor-core kernels
+    runs out after a short limit; the kernels free their tensor memory and
+    return, status() reports TS_ERR_TIMEOUT once, and with the stall lifted
+    the same plan and context transform correctly again."""
+    import time
+    from turing_sphere_b200._lib import TS_ERR_TIMEOUT, TsError
+    lmax, nlat, nphi = 31, 32, 64
+    plan = tc_plan(device, lmax, nlat, nphi)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = scaled_spectrum(lmax, lmax, 7)
+    plan.testStall(True, wait_limit=4096)
+    t0 = time.perf_counter()
+    plan.synth(q)
+    plan.analys(ref.synth(q.astype(np.float64)).astype(np.float32))
+    assert time.perf_counter() - t0 < 30.0
+    with pytest.raises(TsError) as ei:
+        plan.status()
+    assert ei.value.status == TS_ERR_TIMEOUT
+    plan.status()  # reported once
+    plan.testStall(False)
+    s_cpu = ref.synth(q.astype(np.float64))
+    assert O.rel_l2(plan.synth(q), s_cpu) < TOL
+    s32 = s_cpu.astype(np.float32)
+    assert O.rel_l2(plan.analys(s32), ref.analys(s32.astype(np.float64))) < TOL
+    plan.status()
+    fp32 = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi), {"precision": "fp32"})
+    with pytest.raises(TsError):
+        fp32.testStall(True)

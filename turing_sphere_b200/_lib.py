@@ -97,6 +97,7 @@ SIGNATURES = {
     "ts_sht_fourier_analys_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_leg_analys_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_wimage_bytes": (C.c_size_t, [vp, i32]),
+    "ts_sht_plan_test_stall": (i32, [vp, i32, C.c_uint]),
     "ts_sht_synth_adjoint_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_analys_adjoint_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_fourier_analys_w_dev": (i32, [vp, vp, vp, i32, vp]),

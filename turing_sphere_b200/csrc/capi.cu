@@ -321,6 +321,17 @@ int ts_sht_plan_info(ts_plan p, ts_plan_info *info) {
   return TS_OK;
 }
 
+int ts_sht_plan_test_stall(ts_plan p, int stall_copies, unsigned wait_limit) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
+  TS_REQUIRE(p->tc != nullptr, TS_ERR_UNSUPPORTED, "FP32 plans have no bounded waits");
+  TS_CUDA(cudaSetDevice(ctx->device));
+  TS_CUDA(cudaStreamSynchronize(ctx->stream));
+  ts_tc_set_fault(p, stall_copies, wait_limit);
+  TS_API_END(ctx)
+}
+
 int ts_sht_plan_status(ts_plan p) {
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN

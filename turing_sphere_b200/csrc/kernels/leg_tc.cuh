@@ -195,6 +195,7 @@ struct TsTcPipe {
   unsigned long long epi;    // the 4 epilogue warps' own barrier
   unsigned long long drain;  // the MMA warp's last commit before exit
   unsigned tmem;
+  unsigned limit;            // polls of a bounded wait
   int bad;
   int epi_go[2];  // per accumulator buffer: the epilogue warps proceed (1) or leave (0)
 };
@@ -227,8 +228,9 @@ TS_DEV void ts_epi_bar_all() {
   asm volatile("bar.sync 3, 256;" ::: "memory");
 }
 
-TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S) {
+TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S, const TsTcTab &tc) {
   if (threadIdx.x == 0) {
+    pp->limit = tc.wait_limit ? tc.wait_limit : TS_TC_WAIT_LIMIT;
     for (int s = 0; s < S; s++) {
       ts_mbar_init(&pp->full[s], 1);
       ts_mbar_init(&pp->ready[s], 4);
@@ -302,7 +304,7 @@ TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes
   int i = 0;
   for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x, i++) {
     const int b = i & 1;
-    if (i >= 2 && !ts_mbar_wait(&pp->acc_empty[b], ((i >> 1) - 1) & 1, TS_TC_WAIT_LIMIT)) {
+    if (i >= 2 && !ts_mbar_wait(&pp->acc_empty[b], ((i >> 1) - 1) & 1, pp->limit)) {
       ts_tc_flag(pp);
       return;
     }
@@ -313,7 +315,7 @@ TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes
     for (int t_ = 0; t_ < T; t_++, g++) {
       const int s = (int)(g % S);
       const unsigned use = (unsigned)(g / S);
-      if (!ts_mbar_wait(&pp->ready[s], use & 1, TS_TC_WAIT_LIMIT)) {
+      if (!ts_mbar_wait(&pp->ready[s], use & 1, pp->limit)) {
         ts_tc_flag(pp);
         return;
       }
@@ -353,7 +355,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
       for (int t_ = 0; t_ < T; t_++, g++) {
         const int s = (int)(g % S);
         const unsigned use = (unsigned)(g / S);
-        if (!ts_mbar_wait(&pp->full[s], use & 1, TS_TC_WAIT_LIMIT)) {
+        if (!ts_mbar_wait(&pp->full[s], use & 1, pp->limit)) {
           ts_tc_flag(pp);
           return;
         }
@@ -365,7 +367,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
       }
     }
   } else if (warp == 4) {
-    if (lane == 0) {
+    if (lane == 0 && !sc.tc->stall_copies) {
       long g = 0;
       for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x) {
         const int T = sc.stages(tile);
@@ -374,7 +376,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
         for (; t_ < T; t_++, g++) {
           const int s = (int)(g % S);
           const unsigned use = (unsigned)(g / S);
-          if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, TS_TC_WAIT_LIMIT)) {
+          if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, pp->limit)) {
             ts_tc_flag(pp);
             break;
           }
@@ -389,7 +391,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
       // wait (bounded) for the last use of every slot that was issued
       for (int s = 0; s < S && s < g; s++) {
         const unsigned last = (unsigned)((g - 1 - s) / S);
-        if (!ts_mbar_wait(&pp->full[s], last & 1, TS_TC_WAIT_LIMIT)) ts_tc_flag(pp);
+        if (!ts_mbar_wait(&pp->full[s], last & 1, pp->limit)) ts_tc_flag(pp);
       }
     }
   } else if (warp == 5) {
@@ -397,7 +399,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
       ts_tc_mma_role(smem, pp, S, stage_bytes, tmem, acc_cols, sc);
       // every MMA this thread issued has finished before TMEM is released
       ts_mma_commit(&pp->drain);
-      if (!ts_mbar_wait(&pp->drain, 0, TS_TC_WAIT_LIMIT)) ts_tc_flag(pp);
+      if (!ts_mbar_wait(&pp->drain, 0, pp->limit)) ts_tc_flag(pp);
     }
   } else {
     // one thread waits for the accumulator and tells the other epilogue warps
@@ -406,7 +408,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
       const int b = i & 1;
       if (warp == 6 && lane == 0) {
-        const bool ok = ts_mbar_wait(&pp->acc_full[b], (i >> 1) & 1, TS_TC_WAIT_LIMIT);
+        const bool ok = ts_mbar_wait(&pp->acc_full[b], (i >> 1) & 1, pp->limit);
         if (!ok) ts_tc_flag(pp);
         pp->epi_go[b] = ok && !ts_tc_bad(pp);
       }
@@ -502,7 +504,7 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
   const unsigned stage = 2 * 16384 + 2 * NL * 128;
   TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + 2 * TS_TC_SYN_STAGING);
   const TsSynthSched sc{&tc, t.lmax, t.mmax, q_nfb, NL, tc.nLT, qimg};
-  ts_tc_pipe_init(pp, S);
+  ts_tc_pipe_init(pp, S, tc);
   if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
   ts_tc_fence_before();
   __syncthreads();
@@ -630,7 +632,7 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
   float *sD = reinterpret_cast<float *>(smem + S * stage + (grp > 0 ? ana_stg : 0));
   TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + 2 * ana_stg);
   const TsAnalysSched sc{&tc, t.lmax, t.mmax, w_nfb, ntile, wimg};
-  ts_tc_pipe_init(pp, S);
+  ts_tc_pipe_init(pp, S, tc);
   if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
   ts_tc_fence_before();
   __syncthreads();

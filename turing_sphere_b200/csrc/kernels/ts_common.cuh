@@ -111,13 +111,15 @@ struct TsTcTab {
   const char *anal;         // analysis image
   const long *anal_off;
   int NL, nLT;              // synthesis latitude tile (N of the MMA) and tile count
-  int LTL;                  // analysis l-tile (per parity), <= 256
+  int LTL;                  // analysis l-tile (per parity), <= 128
   int nLC;                  // analysis latitude chunks of 32
   int *err;                 // set to 1 when a bounded wait gives up
   const int *chunk_prefix;  // synthesis k-chunks (both parities) before m, mmax+2 entries
   const int *chunk_m;       // chunk -> m
   const int *chunk_pc;      // chunk -> (parity << 16) | chunk-of-parity
   int nchunks;
+  unsigned wait_limit;      // polls before a bounded wait gives up (0: the default)
+  int stall_copies;         // test hook: the copy warp issues nothing, every wait runs out
 };
 
 // The data operands of the tensor-core Legendre stage, kept in HBM as raw fp32

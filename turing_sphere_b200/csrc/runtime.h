@@ -141,6 +141,7 @@ struct TsTcGeom {
   int NL, nLT, LTL, ntile;
 };
 TsTcGeom ts_tc_geom(ts_plan p);
+void ts_tc_set_fault(ts_plan p, int stall_copies, unsigned wait_limit);
 int ts_tc_ctas(ts_plan p, long ntiles);
 // TC synthesis: fields -> q image (qbuf, or the plan's) -> fm
 void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fm_stride, int nfields,

@@ -214,6 +214,12 @@ void ts_tc_free(ts_plan p) {
 }
 
 const TsTcTab &ts_tc_tab(ts_plan p) { return static_cast<ts_tc_tables *>(p->tc)->tab; }
+
+void ts_tc_set_fault(ts_plan p, int stall_copies, unsigned wait_limit) {
+  TsTcTab &t = static_cast<ts_tc_tables *>(p->tc)->tab;
+  t.stall_copies = stall_copies;
+  t.wait_limit = wait_limit;
+}
 int ts_tc_ntile(ts_plan p) { return static_cast<ts_tc_tables *>(p->tc)->ntile; }
 size_t ts_tc_bytes(ts_plan p) { return p->tc ? static_cast<ts_tc_tables *>(p->tc)->bytes : 0; }
 

@@ -175,6 +175,12 @@ class ShtPlan:
         _lib.check(getattr(_lib.lib(), fn)(self.handle, src_ptr, dst_ptr, batch, stream),
                    self.device.handle)
 
+    def testStall(self, stall: bool, wait_limit: int = 0) -> None:
+        """Failure-detection test hook (tensor-core plans): make the kernels'
+        bounded waits run out (stall) or restore normal operation."""
+        _lib.check(_lib.lib().ts_sht_plan_test_stall(self.handle, 1 if stall else 0, wait_limit),
+                   self.device.handle)
+
     def status(self) -> None:
         """Raise TsError(TS_ERR_TIMEOUT) if a tensor-core kernel gave up a wait."""
         _lib.check(_lib.lib().ts_sht_plan_status(self.handle), self.device.handle)
