@@ -246,6 +246,82 @@ TS_DEV void ts_f2_forward(float2 *b, const float2 *twq) {
   }
 }
 
+// ts_f2_inverse whose second phase writes z straight to the grid rows
+// (16 consecutive n2 per half-warp: 128-byte runs), skipping the staging of
+// the result in shared memory
+template <class C, class LatOf>
+TS_DEV void ts_f2_inverse_out(float2 *b, const float2 *twq, float *__restrict__ dst, int nphi,
+                              LatOf lat_of) {
+  const int tid = threadIdx.x;
+  {
+    const int r = tid / C::P, k1 = tid - r * C::P;
+    float2 *row = b + r * C::RP;
+    float2 x[C::Q];
+#pragma unroll
+    for (int k2 = 0; k2 < C::Q; k2++) x[k2] = row[k1 + C::P * k2];
+    ts_dft<C::Q, +1>(x);
+#pragma unroll
+    for (int n2 = 1; n2 < C::Q; n2++) x[n2] = c_mul(x[n2], twq[n2 * C::P1 + k1]);
+    __syncthreads();
+#pragma unroll
+    for (int n2 = 0; n2 < C::Q; n2++) row[n2 * C::P1 + k1] = x[n2];
+    __syncthreads();
+  }
+  if (tid < C::Q * C::R) {
+    const int r = tid / C::Q, n2 = tid - r * C::Q;
+    const int lat = lat_of(r);
+    const float2 *row = b + r * C::RP;
+    float2 x[C::P];
+#pragma unroll
+    for (int k1 = 0; k1 < C::P; k1++) x[k1] = row[n2 * C::P1 + k1];
+    ts_dft<C::P, +1>(x);
+    if (lat >= 0) {
+      float2 *out = reinterpret_cast<float2 *>(dst + (long)lat * nphi) + n2;
+#pragma unroll
+      for (int n1 = 0; n1 < C::P; n1++) out[C::Q * n1] = x[n1];
+    }
+  }
+}
+
+// ts_f2_forward whose first phase reads z straight from the grid rows
+template <class C, class LatOf>
+TS_DEV void ts_f2_forward_in(float2 *b, const float2 *twq, const float *__restrict__ src, int nphi,
+                             LatOf lat_of) {
+  const int tid = threadIdx.x;
+  if (tid < C::Q * C::R) {
+    const int r = tid / C::Q, n2 = tid - r * C::Q;
+    const int lat = lat_of(r);
+    float2 x[C::P];
+    if (lat >= 0) {
+      const float2 *in = reinterpret_cast<const float2 *>(src + (long)lat * nphi) + n2;
+#pragma unroll
+      for (int n1 = 0; n1 < C::P; n1++) x[n1] = in[C::Q * n1];
+    } else {
+#pragma unroll
+      for (int n1 = 0; n1 < C::P; n1++) x[n1] = make_float2(0.f, 0.f);
+    }
+    ts_dft<C::P, -1>(x);
+#pragma unroll
+    for (int k1 = 1; k1 < C::P; k1++) x[k1] = c_mul(x[k1], c_conj(twq[n2 * C::P1 + k1]));
+    float2 *row = b + r * C::RP;
+#pragma unroll
+    for (int k1 = 0; k1 < C::P; k1++) row[n2 * C::P1 + k1] = x[k1];
+  }
+  __syncthreads();
+  {
+    const int r = tid / C::P, k1 = tid - r * C::P;
+    float2 *row = b + r * C::RP;
+    float2 x[C::Q];
+#pragma unroll
+    for (int n2 = 0; n2 < C::Q; n2++) x[n2] = row[n2 * C::P1 + k1];
+    ts_dft<C::Q, -1>(x);
+    __syncthreads();
+#pragma unroll
+    for (int k2 = 0; k2 < C::Q; k2++) row[k1 + C::P * k2] = x[k2];
+    __syncthreads();
+  }
+}
+
 // Z of the synthesis for the CTA's rows from the spectra src[k*nlat + lat]
 // of one field.  lat_of(r) < 0 marks a row without a latitude (zeros).
 // Item i is the pair (k, H-k), k = i / R, of row i % R: consecutive threads
@@ -439,8 +515,7 @@ ts_f2_synth(TsFftTab ft, const float2 *__restrict__ fm, long fm_stride, float *_
   ts_f2_twq<C>(twq, ft);
   ts_f2_pack<C>(b, fm + f * fm_stride, ft, rows);
   __syncthreads();
-  ts_f2_inverse<C>(b, twq);
-  ts_f2_store_rows<C>(b, spat + f * spat_stride, ft.nphi, rows);
+  ts_f2_inverse_out<C>(b, twq, spat + f * spat_stride, ft.nphi, rows);
 }
 
 // spat[field][lat][phi] -> g[field][m][lat].  grid = (ceil(nlat/R), fields).
@@ -455,9 +530,8 @@ ts_f2_analys(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
   const long f = blockIdx.y;
   const TsF2Rows<C, false> rows{(int)blockIdx.x * R, ft.nlat, 0};
   ts_f2_twq<C>(twq, ft);
-  ts_f2_load_rows<C>(b, spat + f * spat_stride, ft.nphi, rows);
   __syncthreads();
-  ts_f2_forward<C>(b, twq);
+  ts_f2_forward_in<C>(b, twq, spat + f * spat_stride, ft.nphi, rows);
   ts_f2_unpack<C>(b, g + f * g_stride, ft, rows);
 }
 
@@ -474,9 +548,8 @@ ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
   const int lat0 = blockIdx.x * (R / 2);
   const TsF2Rows<C, true> rows{lat0, ft.nlat, nh};
   ts_f2_twq<C>(twq, ft);
-  ts_f2_load_rows<C>(b, spat + f * spat_stride, ft.nphi, rows);
   __syncthreads();
-  ts_f2_forward<C>(b, twq);
+  ts_f2_forward_in<C>(b, twq, spat + f * spat_stride, ft.nphi, rows);
   ts_f2_write_w<C>(b, lat0, f, ft, wq, wimg, nfb, fpb, nlc, nh);
 }
 
