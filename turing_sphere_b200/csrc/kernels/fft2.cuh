@@ -495,10 +495,10 @@ constexpr long ts_f2_smem_bytes(int nb) {
 
 // Resident CTAs per SM asked of the register allocator.  Transform kernels
 // with P <= 24: 1152 threads per SM (<= 56 registers each), else whatever
-// fits.  The fused phase holds two row blocks and the generated program: two
-// CTAs of up to 384 threads per SM (<= 85 registers).
+// fits.  The fused phase keeps every species' P grid points of a row in
+// registers (~170 registers): no limit.
 #define TS_F2_MINB(P, R) ((P) <= 24 ? 1152 / ((P) * (R)) : 1)
-#define TS_F2_PHASE_MINB(P, R) ((P) * (R) <= 384 ? 2 : 1)
+#define TS_F2_PHASE_MINB(P, R) 1
 
 // fm[field][m][lat] -> spat[field][lat][phi].  grid = (ceil(nlat/R), fields),
 // block = P*R.
@@ -565,14 +565,50 @@ ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
 // analysis as the W image, otherwise it writes
 //   gm [inst][NANA][mmax+1][nlat].
 // grid = (ceil(nlat/R) or ceil(nh/(R/2)), instances), block = P*R; shared
-// memory ts_f2_smem_bytes(max(NSYN + NGIN, NANA, 1)).
+// memory ts_f2_smem_bytes(max(NSYN, NANA, 1)).
+// phase 1 of the synthesis for the row block at b: Q-point DFTs over k2,
+// twiddles, transposed store (two barriers)
+template <class C>
+TS_DEV void ts_f2_inv_phase1(float2 *b, const float2 *twq) {
+  const int tid = threadIdx.x;
+  const int r = tid / C::P, k1 = tid - r * C::P;
+  float2 *row = b + r * C::RP;
+  float2 x[C::Q];
+#pragma unroll
+  for (int k2 = 0; k2 < C::Q; k2++) x[k2] = row[k1 + C::P * k2];
+  ts_dft<C::Q, +1>(x);
+#pragma unroll
+  for (int n2 = 1; n2 < C::Q; n2++) x[n2] = c_mul(x[n2], twq[n2 * C::P1 + k1]);
+  __syncthreads();
+#pragma unroll
+  for (int n2 = 0; n2 < C::Q; n2++) row[n2 * C::P1 + k1] = x[n2];
+  __syncthreads();
+}
+
+// phase 2 of the analysis for the row block at b: Q-point DFTs over n2 from
+// the transposed layout, natural store (two barriers)
+template <class C>
+TS_DEV void ts_f2_fwd_phase2(float2 *b) {
+  const int tid = threadIdx.x;
+  const int r = tid / C::P, k1 = tid - r * C::P;
+  float2 *row = b + r * C::RP;
+  float2 x[C::Q];
+#pragma unroll
+  for (int n2 = 0; n2 < C::Q; n2++) x[n2] = row[n2 * C::P1 + k1];
+  ts_dft<C::Q, -1>(x);
+  __syncthreads();
+#pragma unroll
+  for (int k2 = 0; k2 < C::Q; k2++) row[k1 + C::P * k2] = x[k2];
+  __syncthreads();
+}
+
 template <class Prog, int P, int Q, int R, bool PAIRED>
 __global__ void __launch_bounds__(P *R, TS_F2_PHASE_MINB(P, R))
 ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
   using C = TsF2<P, Q, R>;
   constexpr int NSYN = Prog::NSYN, NGIN = Prog::NGIN, NANA = Prog::NANA, NGOUT = Prog::NGOUT;
   constexpr int NIN = NSYN + NGIN;
-  constexpr int NB = NIN > NANA ? (NIN > 0 ? NIN : 1) : (NANA > 0 ? NANA : 1);
+  constexpr int NB = NSYN > NANA ? NSYN : (NANA > 0 ? NANA : 1);
   extern __shared__ float2 ts_smem_f2p[];
   float2 *twq = ts_smem_f2p;
   float2 *buf = twq + C::TWQ;
@@ -584,41 +620,69 @@ ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
 #pragma unroll 1
   for (int s = 0; s < NSYN; s++)
     ts_f2_pack<C>(buf + s * BS, io.fm + (inst * NSYN + s) * io.field, ft, rows);
-#pragma unroll 1
-  for (int gi = 0; gi < NGIN; gi++)
-    ts_f2_load_rows<C>(buf + (NSYN + gi) * BS, io.gin[gi] + inst * io.gin_stride[gi], ft.nphi,
-                       rows);
   __syncthreads();
 #pragma unroll 1
-  for (int s = 0; s < NSYN; s++) ts_f2_inverse<C>(buf + s * BS, twq);
+  for (int s = 0; s < NSYN; s++) ts_f2_inv_phase1<C>(buf + s * BS, twq);
 
-  // the element-wise program: every input of a point is read before its
-  // outputs overwrite the same position of the first NANA blocks
-  const float *prm = io.prm + inst * io.nprm;
-  ts_f2_for_rows<C>([&](int, int r, int n) {
+  // Thread (row r, n2) holds, after the synthesis's P-point DFTs, every
+  // species at the grid points n = Q n1 + n2 (n1 < P): exactly the inputs
+  // of the analysis's first P-point DFTs.  The program runs there, in
+  // registers; grid inputs and outputs move as 128-byte runs (16 lanes of
+  // consecutive n2).
+  if (threadIdx.x < C::Q * C::R) {
+    const int r = threadIdx.x / C::Q, n2 = threadIdx.x - r * C::Q;
     const int lat = rows(r);
-    if (lat < 0) return;
-    const int pos = r * C::RP + n;
-    float in0[NIN > 0 ? NIN : 1], in1[NIN > 0 ? NIN : 1];
+    const float *prm = io.prm + inst * io.nprm;
+    float2 w[NB][P];
 #pragma unroll
-    for (int k = 0; k < NIN; k++) {
-      const float2 z = buf[k * BS + pos];
-      in0[k] = z.x;
-      in1[k] = z.y;
+    for (int s = 0; s < NSYN; s++) {
+      const float2 *row = buf + s * BS + r * C::RP + n2 * C::P1;
+#pragma unroll
+      for (int k1 = 0; k1 < P; k1++) w[s][k1] = row[k1];
+      ts_dft<P, +1>(w[s]);
     }
-    float out0[NANA + NGOUT > 0 ? NANA + NGOUT : 1], out1[NANA + NGOUT > 0 ? NANA + NGOUT : 1];
-    Prog::eval(in0, out0, prm);
-    Prog::eval(in1, out1, prm);
 #pragma unroll
-    for (int k = 0; k < NANA; k++) buf[k * BS + pos] = make_float2(out0[k], out1[k]);
+    for (int n1 = 0; n1 < P; n1++) {
+      const long n = (long)Q * n1 + n2;
+      float in0[NIN > 0 ? NIN : 1], in1[NIN > 0 ? NIN : 1];
 #pragma unroll
-    for (int o = 0; o < NGOUT; o++)
-      reinterpret_cast<float2 *>(io.gout[o] + inst * io.gout_stride[o] + (long)lat * ft.nphi)[n] =
-          make_float2(out0[NANA + o], out1[NANA + o]);
-  });
+      for (int s = 0; s < NSYN; s++) {
+        in0[s] = w[s][n1].x;
+        in1[s] = w[s][n1].y;
+      }
+#pragma unroll
+      for (int gi = 0; gi < NGIN; gi++) {
+        float2 g = make_float2(0.f, 0.f);
+        if (lat >= 0)
+          g = reinterpret_cast<const float2 *>(io.gin[gi] + inst * io.gin_stride[gi] +
+                                               (long)lat * ft.nphi)[n];
+        in0[NSYN + gi] = g.x;
+        in1[NSYN + gi] = g.y;
+      }
+      float out0[NANA + NGOUT > 0 ? NANA + NGOUT : 1], out1[NANA + NGOUT > 0 ? NANA + NGOUT : 1];
+      Prog::eval(in0, out0, prm);
+      Prog::eval(in1, out1, prm);
+#pragma unroll
+      for (int o = 0; o < NANA; o++) w[o][n1] = make_float2(out0[o], out1[o]);
+      if (lat >= 0) {
+#pragma unroll
+        for (int o = 0; o < NGOUT; o++)
+          reinterpret_cast<float2 *>(io.gout[o] + inst * io.gout_stride[o] +
+                                     (long)lat * ft.nphi)[n] = make_float2(out0[NANA + o], out1[NANA + o]);
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < NANA; o++) {
+      ts_dft<P, -1>(w[o]);
+      float2 *row = buf + o * BS + r * C::RP + n2 * C::P1;
+      row[0] = w[o][0];
+#pragma unroll
+      for (int k1 = 1; k1 < P; k1++) row[k1] = c_mul(w[o][k1], c_conj(twq[n2 * C::P1 + k1]));
+    }
+  }
   __syncthreads();
 #pragma unroll 1
-  for (int k = 0; k < NANA; k++) ts_f2_forward<C>(buf + k * BS, twq);
+  for (int k = 0; k < NANA; k++) ts_f2_fwd_phase2<C>(buf + k * BS);
 #pragma unroll 1
   for (int k = 0; k < NANA; k++) {
     if constexpr (PAIRED)

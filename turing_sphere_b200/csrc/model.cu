@@ -451,7 +451,7 @@ void schedule(ts_model m, Program &P, bool is_step) {
       src << "  }\n};\n";
       // two-phase FFT when the row length has a shape and the row blocks fit
       int fP = 0, fQ = 0, fR = 0;
-      const int nb = std::max<int>({(int)(S.size() + gin.size()), (int)A.size(), 1});
+      const int nb = std::max<int>({(int)S.size(), (int)A.size(), 1});
       if (ts_f2_shape(p, &fP, &fQ)) fR = ts_f2_phase_rows(p, nb, &st.smem);
       const bool tcw = p->precision != TS_PREC_FP32 && fR && !A.empty();
       if (fR) {

@@ -409,16 +409,18 @@ size_t ts_f2_bytes(int P, int Q, int R, int nb) {
   return sizeof(float2) * ((size_t)Q * (P + 1) + (size_t)nb * R * RP);
 }
 
-// rows per phase CTA with nb row blocks: 16 while two CTAs fit on an SM,
-// else the largest of 8, 4 that fits at all (0: none does)
+// rows per phase CTA with nb row blocks: the largest of 16, 8, 4 that fits
+// (0: none does)
 int ts_f2_phase_rows(ts_plan p, int nb, size_t *smem) {
   int P, Q;
   if (!ts_f2_shape(p, &P, &Q)) return 0;
   const size_t cap = p->ctx->smem_optin;
+  int want = 0;  // TS_PHASE_ROWS (16, 8 or 4) tunes it, like the reference's SHT_* knobs
+  if (const char *e = getenv("TS_PHASE_ROWS")) want = atoi(e);
   for (int R : {16, 8, 4}) {
+    if (want && R != want) continue;
     const size_t b = ts_f2_bytes(P, Q, R, nb);
     if (P * R > 1024 || b > cap) continue;
-    if (R == 16 && 2 * (b + 1024) > cap + 1024) continue;
     *smem = b;
     return R;
   }
