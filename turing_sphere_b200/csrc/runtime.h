@@ -121,7 +121,7 @@ int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem);
 // the Stockham kernels run), its shared memory, and the rows of a phase CTA
 bool ts_f2_shape(ts_plan p, int *P, int *Q);
 size_t ts_f2_bytes(int P, int Q, int R, int nb);
-int ts_f2_phase_rows(ts_plan p, int nb, size_t *smem);
+int ts_f2_phase_rows(ts_plan p, int nb, int batch, size_t *smem);
 // raise a kernel's dynamic shared-memory limit on `device` (once per size)
 void ts_allow_smem(const void *fn, int device, size_t bytes);
 void ts_init_tables(ts_plan p);

@@ -410,21 +410,24 @@ size_t ts_f2_bytes(int P, int Q, int R, int nb) {
 }
 
 // rows per phase CTA with nb row blocks: the largest of 16, 8, 4 that fits
-// (0: none does)
-int ts_f2_phase_rows(ts_plan p, int nb, size_t *smem) {
+// and still gives every SM a CTA for `batch` instances (0: none fits)
+int ts_f2_phase_rows(ts_plan p, int nb, int batch, size_t *smem) {
   int P, Q;
   if (!ts_f2_shape(p, &P, &Q)) return 0;
   const size_t cap = p->ctx->smem_optin;
   int want = 0;  // TS_PHASE_ROWS (16, 8 or 4) tunes it, like the reference's SHT_* knobs
   if (const char *e = getenv("TS_PHASE_ROWS")) want = atoi(e);
+  // fewer rows per CTA while the grid would leave SMs idle (a small batch)
+  int chosen = 0;
   for (int R : {16, 8, 4}) {
     if (want && R != want) continue;
     const size_t b = ts_f2_bytes(P, Q, R, nb);
     if (P * R > 1024 || b > cap) continue;
+    chosen = R;
     *smem = b;
-    return R;
+    if (want || (long)batch * ((p->nlat + R - 1) / R) >= p->ctx->sm_count) break;
   }
-  return 0;
+  return chosen;
 }
 
 void ts_allow_smem(const void *fn, int device, size_t bytes) {
@@ -467,6 +470,15 @@ void f2_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb, char *w
 }
 }  // namespace
 
+namespace {
+// rows of a standalone FFT CTA: the tuned choice, else the default unless a
+// small batch would leave SMs idle
+int pick_rows(ts_plan p, int nf, int rlo, int rhi) {
+  if (p->fft_rows) return p->fft_rows == rlo ? rlo : rhi;
+  return (long)nf * ((p->nlat + rhi - 1) / rhi) < p->ctx->sm_count ? rlo : rhi;
+}
+}  // namespace
+
 int ts_f2_rows(ts_plan p) {
   if (p->fourier != TS_FOURIER_FFT) return 0;
   switch (p->fft.H) {
@@ -486,7 +498,7 @@ bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, i
   switch (p->fft.H) {
 #define TS_F2_CASE(h, pp, qq, rlo, rhi)                                     \
   case h:                                                                   \
-    if (p->fft_rows == rlo)                                                 \
+    if (pick_rows(p, nf, rlo, rhi) == rlo)                                  \
       f2_analys_w<pp, qq, rlo>(p, spat, ss, nf, fpb, wimg, s);              \
     else                                                                    \
       f2_analys_w<pp, qq, rhi>(p, spat, ss, nf, fpb, wimg, s);              \
@@ -504,7 +516,7 @@ void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, 
     switch (p->fft.H) {
 #define TS_F2_CASE(h, pp, qq, rlo, rhi)                                         \
   case h:                                                                       \
-    return p->fft_rows == rlo ? f2_synth<pp, qq, rlo>(p, fm, fs, spat, ss, nf, s) \
+    return pick_rows(p, nf, rlo, rhi) == rlo ? f2_synth<pp, qq, rlo>(p, fm, fs, spat, ss, nf, s) \
                               : f2_synth<pp, qq, rhi>(p, fm, fs, spat, ss, nf, s);
       TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
@@ -531,7 +543,7 @@ void ts_launch_fourier_analys(ts_plan p, const float *spat, long ss, float2 *g, 
     switch (p->fft.H) {
 #define TS_F2_CASE(h, pp, qq, rlo, rhi)                                        \
   case h:                                                                      \
-    return p->fft_rows == rlo ? f2_analys<pp, qq, rlo>(p, spat, ss, g, gs, nf, s) \
+    return pick_rows(p, nf, rlo, rhi) == rlo ? f2_analys<pp, qq, rlo>(p, spat, ss, g, gs, nf, s) \
                               : f2_analys<pp, qq, rhi>(p, spat, ss, g, gs, nf, s);
       TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
