@@ -147,10 +147,14 @@ struct TsAnalysStore {
 };
 
 // per_cta <= F fields per CTA (a model groups whole instances per CTA).
+// lchunk > 0 splits each m's degrees over CTAs (blockIdx.z: degrees
+// i = l - m in [z*lchunk, (z+1)*lchunk), lchunk a multiple of 2P): a CTA
+// advances the recurrence without reducing up to its chunk, so small grids
+// still fill the GPU; 0 = one CTA per m.
 template <int F, int K, int P, class Epi>
 __global__ void __launch_bounds__(256)
 ts_leg_analys_f32(TsLegTab t, const float2 *__restrict__ g, long g_stride, Epi epi,
-                  int nfields, int per_cta) {
+                  int nfields, int per_cta, int lchunk) {
   constexpr int N = 4 * P * F;  // (p, comp4, f) values per span
   constexpr int CNT = N >= 32 ? N / 32 : 1;
   extern __shared__ float ts_smem_la[];
@@ -158,6 +162,9 @@ ts_leg_analys_f32(TsLegTab t, const float2 *__restrict__ g, long g_stride, Epi e
   const int f0 = blockIdx.y * per_cta;
   const int nf = min(per_cta, nfields - f0);
   const int Km = t.lmax - m + 1;
+  const int c_begin = lchunk ? (int)blockIdx.z * lchunk : 0;
+  const int c_end = lchunk ? min(Km, c_begin + lchunk) : Km;
+  if (c_begin >= Km) return;
   const long base = ts_lm_base(t.lmax, m);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int W = blockDim.x >> 5;
@@ -203,7 +210,30 @@ ts_leg_analys_f32(TsLegTab t, const float2 *__restrict__ g, long g_stride, Epi e
     y1v[k] = (m < t.lmax) ? sab[1].x * ct * y0v[k] : 0.0f;
   }
 
-  for (int i0 = 0; i0 < Km; i0 += 2 * P) {
+  for (int i0 = 0; i0 < c_begin; i0 += 2 * P) {  // recurrence only, up to the chunk
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      const int i = i0 + 2 * p;
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        if (nyv[k] != 0 && fabsf(y0v[k]) > TS_RESCALE_THR) {
+          nyv[k] += 1;
+          y0v[k] *= TS_INV_SCALE;
+          y1v[k] *= TS_INV_SCALE;
+        }
+      if (i + 2 < Km) {
+        const float2 a0 = sab[i + 2];
+        const float2 a1 = (i + 3 < Km) ? sab[i + 3] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const float t0 = a0.x * ctv[k] * y1v[k] + a0.y * y0v[k];
+          y1v[k] = a1.x * ctv[k] * t0 + a1.y * y1v[k];
+          y0v[k] = t0;
+        }
+      }
+    }
+  }
+  for (int i0 = c_begin; i0 < c_end; i0 += 2 * P) {
     float v[N];
 #pragma unroll
     for (int j = 0; j < N; j++) v[j] = 0.f;
@@ -257,7 +287,7 @@ ts_leg_analys_f32(TsLegTab t, const float2 *__restrict__ g, long g_stride, Epi e
     for (int j = tid; j < 4 * P; j += blockDim.x) {
       const int p = j >> 2, c = j & 3;
       const int i = i0 + 2 * p + (c >> 1);
-      if (i < Km) epi(base + i, c & 1, res + (p * 4 + c) * F, f0, nf, F);
+      if (i < c_end) epi(base + i, c & 1, res + (p * 4 + c) * F, f0, nf, F);
     }
     __syncthreads();
   }

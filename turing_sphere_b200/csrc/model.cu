@@ -778,8 +778,10 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
           const int ctas = ts_tc_ctas(p, (long)(p->mmax + 1) * 2 * ntile * w_nfb);
           TS_CUDA(cudaLaunchKernel((const void *)s.kern, dim3(ctas), dim3(TS_TC_THREADS), args, s.smem, st));
         } else {
-          void *args[] = {&leg, &g, &gs, &epi, &nfields, &per_cta};
-          dim3 grid(p->mmax + 1, (nfields + per_cta - 1) / per_cta);
+          const int nfb = (nfields + per_cta - 1) / per_cta;
+          int lchunk = ts_analys_lchunk(p, nfb);
+          void *args[] = {&leg, &g, &gs, &epi, &nfields, &per_cta, &lchunk};
+          dim3 grid(p->mmax + 1, nfb, lchunk ? (p->lmax + lchunk) / lchunk : 1);
           TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(32 * s.W), args, s.smem, st));
         }
         break;

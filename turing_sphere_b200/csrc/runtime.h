@@ -114,6 +114,7 @@ void ts_launch_leg_synth_plain(ts_plan p, const TsFields &q, float2 *fm, long fm
 // warps W; groups = fields handled per CTA (a multiple of `per_inst`)
 void ts_analys_shape(ts_plan p, int nfields, int per_inst, int *F, int *K, int *W, int *per_cta);
 size_t ts_analys_smem(ts_plan p, int F, int W);
+int ts_analys_lchunk(ts_plan p, int nfb);
 // rows per Fourier CTA for a kernel holding `nrows` rows per warp
 int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem);
 // warp-register FFT: R1 = H/32 (0 = not applicable) and rows per CTA

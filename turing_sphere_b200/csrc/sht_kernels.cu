@@ -216,10 +216,13 @@ void leg_analys_t(ts_plan p, int W, const float2 *g, long gs, float2 *q, long qs
                   cudaStream_t s) {
   constexpr int P = 2;
   constexpr int N = 4 * P * F;
-  dim3 grid(p->mmax + 1, (nf + F - 1) / F);
+  const int nfb = (nf + F - 1) / F;
+  const int lchunk = ts_analys_lchunk(p, nfb);
+  dim3 grid(p->mmax + 1, nfb, lchunk ? (p->lmax + lchunk) / lchunk : 1);
   const size_t smem = sizeof(float2) * (p->lmax + 1) + sizeof(float) * (size_t)(W * N + N);
   TsAnalysStore epi{q, qs};
-  ts_leg_analys_f32<F, K, P, TsAnalysStore><<<grid, 32 * W, smem, s>>>(p->leg, g, gs, epi, nf, F);
+  ts_leg_analys_f32<F, K, P, TsAnalysStore><<<grid, 32 * W, smem, s>>>(p->leg, g, gs, epi, nf, F,
+                                                                       lchunk);
   TS_CUDA(cudaGetLastError());
 }
 
@@ -333,6 +336,18 @@ void ts_analys_shape(ts_plan p, int nfields, int per_inst, int *F, int *K, int *
   }
   *F = f;
   *per_cta = groups * per_inst;
+}
+
+// degrees per FP32-analysis CTA: 0 (all of one m) unless the grid of
+// (mmax+1) x nfb CTAs would leave SMs idle; then chunks of a multiple of 4
+// degrees so that about two CTAs per SM exist
+int ts_analys_lchunk(ts_plan p, int nfb) {
+  const long ctas = (long)(p->mmax + 1) * nfb;
+  if (ctas >= p->ctx->sm_count) return 0;
+  const long want = (2L * p->ctx->sm_count + ctas - 1) / ctas;  // chunks per m
+  int len = (int)((p->lmax + 1 + want - 1) / want);
+  len = std::max(8, (len + 3) & ~3);
+  return len >= p->lmax + 1 ? 0 : len;
 }
 
 size_t ts_analys_smem(ts_plan p, int F, int W) {
