@@ -1,0 +1,59 @@
+"""The solver-benchmark runner (scripts/bench.ts of the reference) end to end
+on a small grid: the --json object's shape, the dump file and its digest, and
+that a second run from the same spec reproduces the digest bit for bit."""
+import json
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from turing_sphere_b200.digest import digestOf
+from turing_sphere_b200.layout import gridForLmax
+from turing_sphere_b200.registry import mModelByKey
+from turing_sphere_b200.runspec import parseArgs
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(args):
+    out = subprocess.run([sys.executable, "-m", "turing_sphere_b200.run", *args],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    return out.stdout
+
+
+def test_json_and_dump(tmp_path):
+    dump = tmp_path / "state.json"
+    args = ["--preset", "schnak-spots", "--lmax", "31", "--steps", "40", "--warmup", "3",
+            "--seed", "5", "--batch", "8", "--json", "--dump-state", str(dump)]
+    j = json.loads(_run(args))
+    assert list(j) == ["command", "spec", "model", "backend", "grid", "compiled", "digest",
+                       "throughput", "latency", "state"]
+    nlat, nphi = gridForLmax(31, mModelByKey(j["model"]).pdeg)
+    assert j["grid"] == {"lmax": 31, "nlat": nlat, "nphi": nphi, "nlm": 32 * 33 // 2}
+    assert j["compiled"]["opsPerStep"] >= 1 and j["compiled"]["kernels"] >= 1
+    assert j["throughput"]["batch"] == 8 and j["throughput"]["msPerStep"] > 0
+    assert j["latency"]["minMs"] <= j["latency"]["medianMs"] <= j["latency"]["p95Ms"]
+    assert j["state"]["finite"] and j["state"]["steps"] == 3 + 40 + 40
+    # the command it prints parses back to the same spec
+    assert parseArgs(j["command"].split()[3:]).as_json() == j["spec"]
+    d = json.loads(dump.read_text())
+    assert d["digest"] == j["digest"] and d["command"] == j["command"]
+    st = np.asarray(d["state"], dtype=np.float32)
+    assert st.size == 2 * j["grid"]["nlm"]
+    assert digestOf(st, j["digest"]["fourier"], j["digest"]["adapter"]) == d["digest"]
+    again = json.loads(_run(args))
+    assert again["digest"] == j["digest"]
+
+
+def test_text_output():
+    out = _run(["--preset", "allencahn", "--lmax", "15", "--steps", "10", "--warmup", "0",
+                "--digest"])
+    assert "ms/step" in out and "state after 10 steps from seed 1:" in out and "n=" in out
+
+
+def test_bad_option_exits_2():
+    out = subprocess.run([sys.executable, "-m", "turing_sphere_b200.run", "--nope", "1"],
+                         capture_output=True, text=True, timeout=60)
+    assert out.returncode == 2 and "unknown option(s): --nope" in out.stderr
