@@ -47,3 +47,30 @@ def test_spec_json_shape():
     j = s.as_json()
     assert list(j) == ["preset", "lmax", "seed", "steps", "warmup", "params"]
     assert j["params"] == resolvePreset("allencahn")[1]
+
+
+def test_compare_dump_files(tmp_path):
+    """The --check diff of two dump files: same spec and close states pass,
+    a changed parameter or a perturbed state fails."""
+    import json
+
+    import numpy as np
+
+    from turing_sphere_b200 import compare
+    from turing_sphere_b200.digest import digestOf
+
+    spec = parseArgs(["--lmax", "7", "--steps", "5"]).as_json()
+    st = np.random.default_rng(0).standard_normal(72).astype(np.float32)
+
+    def dump(name, state, sp=spec):
+        p = tmp_path / name
+        p.write_text(json.dumps({"command": "", "spec": sp, "state": [float(v) for v in state],
+                                 "digest": digestOf(state, "fft", "x")}))
+        return str(p)
+
+    a = dump("a.json", st)
+    assert compare.main([a, dump("b.json", st * (1 + 1e-5))]) == 0
+    assert compare.main([a, dump("c.json", st + 0.1)]) == 1
+    other = dict(spec, params=dict(spec["params"], dt=0.01))
+    assert compare.main([a, dump("d.json", st, other)]) == 1
+    assert compare.main([a]) == 2
