@@ -49,6 +49,11 @@ def parse():
     ap.add_argument("--only", choices=["all", "sht", "imex"], default="all",
                     help="sht: the timed transform pairs alone; imex: the model steps alone "
                          "(short runs for a profiler's launch list)")
+    ap.add_argument("--skip-config1", action="store_true",
+                    help="with --only imex: leave out the 2000-step single-instance runs")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="plans keep their default kernel shapes (no tuning launches, so a "
+                         "profiler's launch skip count lands on the timed kernels)")
     return ap.parse_args()
 
 
@@ -541,20 +546,22 @@ def main():
     torch.cuda.set_stream(stream)
     dev.set_stream(stream.cuda_stream)
     cfg = ShtConfig(lmax, lmax, nlat, nphi)
-    plan = ShtPlan.create(dev, cfg, {"precision": args.precision, "autotune": True})
-    plain = ShtPlan.create(dev, cfg, {"precision": "fp32", "autotune": True})
+    tune = not args.no_autotune
+    plan = ShtPlan.create(dev, cfg, {"precision": args.precision, "autotune": tune})
+    plain = ShtPlan.create(dev, cfg, {"precision": "fp32", "autotune": tune})
     nlm = plan.nlm
 
     if args.only == "imex":
         ni = args.imex_instances
         ims, launches, ok = time_imex(dev, plan, ni, args.imex_steps, max(3, args.warmup), stream)
-        c1 = {g: time_imex_config1(dev, stream, "fp32", graphs=g) for g in (True, False)}
+        c1 = {} if args.skip_config1 else {
+            g: time_imex_config1(dev, stream, "fp32", graphs=g) for g in (True, False)}
         if rank == 0:
             print(json.dumps({"only": "imex", "instances": ni, "launches_per_step": launches,
                               "ms_per_step": ims / args.imex_steps, "finite": ok,
                               "value": world * ni * args.imex_steps / (ims / 1e3),
                               "unit": "instance-steps/s",
-                              "config1_steps_per_s": {"graphs": c1[True], "eager": c1[False]}}),
+                              "config1_steps_per_s": {"graphs": c1.get(True), "eager": c1.get(False)}}),
                   flush=True)
         return finish(plan, plain, dev, world)
 
@@ -631,28 +638,42 @@ def main():
         sp_b = 4.0 * nlat * nphi * B
         alg_bytes = {"legSynth": nlm_b + fm_b, "fourSynth": fm_b + sp_b,
                      "fourAnalys": sp_b + fm_b, "fourAnalysW": sp_b + fm_b,
-                     "legAnalys": fm_b + nlm_b, "legAnalysW": fm_b + nlm_b}[name]
+                     "legAnalys": fm_b + nlm_b, "legAnalysW": fm_b + nlm_b}
         leg_flop = 2.0 * nlm * nlat * B  # complex x real FMA per (l, m, latitude pair)
-        dur = stage_ms[name] / 1e3
-        if name.startswith("leg"):
-            passes = 3 if args.precision != "fp32" else 1
-            roof = {"kernel": name, "bound": "tensor", "achieved": leg_flop / dur / 1e12,
-                    "peak": bf16 / 2, "unit": "TFLOP/s",
-                    "frac": leg_flop / dur / 1e12 / (bf16 / 2), "traffic": None,
-                    "peak_source": f"{src} bf16_tflops / 2 (dense TF32 rate, of measured)",
-                    "algorithmic_flop": leg_flop,
-                    "tensor_pipe_tflops": passes * leg_flop / dur / 1e12,
-                    "note": "achieved counts algorithmic flops; the tensor pipe runs "
-                            f"{passes} split-TF32 passes of them"}
-        else:
-            roof = {"kernel": name, "bound": "hbm", "achieved": alg_bytes / dur / 1e9,
-                    "peak": hbm, "unit": "GB/s", "frac": alg_bytes / dur / 1e9 / hbm,
-                    "traffic": None, "peak_source": f"{src} hbm_gbs (of measured)",
-                    "algorithmic_bytes": alg_bytes}
+        passes = 3 if args.precision != "fp32" else 1
+        of = "of measured" if src == "measured" else "of fallback"
+
+        def stage_roof(st):
+            """Roofline of one stage: the larger of its HBM floor (algorithmic
+            bytes / bandwidth) and, for a Legendre stage, its tensor floor
+            (the split-TF32 passes of its flops / the dense TF32 rate)."""
+            dur = stage_ms[st] / 1e3
+            t_hbm = alg_bytes[st] / (hbm * 1e9)
+            t_tc = passes * leg_flop / (bf16 / 2 * 1e12) if st.startswith("leg") else 0.0
+            if t_tc > t_hbm:
+                return {"kernel": st, "bound": "tensor", "achieved": leg_flop / dur / 1e12,
+                        "peak": bf16 / 2, "unit": "TFLOP/s",
+                        "frac": leg_flop / dur / 1e12 / (bf16 / 2),
+                        "peak_source": f"bf16_tflops / 2, the dense TF32 rate ({of})",
+                        "algorithmic_flop": leg_flop}
+            r = {"kernel": st, "bound": "hbm", "achieved": alg_bytes[st] / dur / 1e9,
+                 "peak": hbm, "unit": "GB/s", "frac": alg_bytes[st] / dur / 1e9 / hbm,
+                 "peak_source": f"hbm_gbs ({of})", "algorithmic_bytes": alg_bytes[st]}
+            if st.startswith("leg"):
+                r["tensor_floor_us"] = t_tc * 1e6
+                r["hbm_floor_us"] = t_hbm * 1e6
+                r["tensor_pipe_tflops"] = passes * leg_flop / dur / 1e12
+                r["note"] = (f"HBM-bound: moving its inputs and outputs takes longer than its "
+                             f"{passes} split-TF32 tensor passes at the dense TF32 rate")
+            return r
+
+        roof = stage_roof(name)
         roof["traffic"] = profiled_traffic(name)
         roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                   "launch (profiles/sht_pair_lmax255_b256_kernels.txt)")
         roof["stage_ms"] = stage_ms
+        roof["stages"] = {st: {k: v for k, v in stage_roof(st).items()
+                               if k in ("bound", "achieved", "unit", "frac")} for st in stages}
         cpu = cpu_baseline(lmax, nlat, nphi, budget_s=10.0, threads=0)
         line = {
             "metric": METRIC, "value": value, "unit": "SHT pairs/s", "n_gpus": world,
