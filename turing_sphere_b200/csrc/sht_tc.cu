@@ -260,9 +260,12 @@ int ts_tc_ctas(ts_plan p, long ntiles) {
 namespace {
 
 // Q (fields) -> raw fp32 synthesis image; grid = (nchunks, q_nfb), block =
-// 256: warp -> 8 fields, lane -> k (coalesced 128-byte image rows)
+// 256: warp -> 8 fields, lane -> k (coalesced 128-byte image rows).  A thread
+// issues the loads of all its 8 fields before its first store, so 8 loads
+// per thread are in flight instead of one.
 __global__ void ts_k_qimage(TsLegTab t, TsTcTab tc, TsFields q, int nfields, char *img,
                             int nfb) {
+  constexpr int NF = TS_TC_FIELDS / 8;  // fields per thread
   const int c = blockIdx.x, fb = blockIdx.y;
   const int m = tc.chunk_m[c], pc = tc.chunk_pc[c];
   const int par = pc >> 16, cc = pc & 0xffff;
@@ -271,12 +274,18 @@ __global__ void ts_k_qimage(TsLegTab t, TsTcTab tc, TsFields q, int nfields, cha
   char *blk = img + ((long)c * nfb + fb) * 16384;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int j = cc * TS_TC_KCH + lane;
-  for (int fl = warp; fl < TS_TC_FIELDS; fl += 8) {
-    const int f = fb * TS_TC_FIELDS + fl;
-    float2 v = make_float2(0.f, 0.f);
-    if (f < nfields && j < kp) v = ts_field(q, f)[base + par + 2 * j];
-    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl, lane)) = v.x;
-    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl + 1, lane)) = v.y;
+  float2 v[NF];
+#pragma unroll
+  for (int i = 0; i < NF; i++) {
+    const int f = fb * TS_TC_FIELDS + warp + 8 * i;
+    v[i] = make_float2(0.f, 0.f);
+    if (f < nfields && j < kp) v[i] = __ldg(ts_field(q, f) + base + par + 2 * j);
+  }
+#pragma unroll
+  for (int i = 0; i < NF; i++) {
+    const int fl = warp + 8 * i;
+    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl, lane)) = v[i].x;
+    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl + 1, lane)) = v[i].y;
   }
 }
 
@@ -292,16 +301,23 @@ __global__ void ts_k_wimage(TsLegTab t, const float2 *g, long gs, int nfields, i
   const float w = live ? t.wq[lat] : 0.f;
   const int south = t.nlat - 1 - lat;
   char *blk = img + ((((long)m * nfb + fb) * 2 + par) * nlc + c) * 16384;
-  for (int fl = warp; fl < TS_TC_FIELDS; fl += 8) {
-    const int f = fb * fpb + fl;
-    float2 gn = make_float2(0.f, 0.f), gsv = make_float2(0.f, 0.f);
+  constexpr int NF = TS_TC_FIELDS / 8;  // fields per thread, loaded before any store
+  float2 gn[NF], gsv[NF];
+#pragma unroll
+  for (int i = 0; i < NF; i++) {
+    const int fl = warp + 8 * i, f = fb * fpb + fl;
+    gn[i] = gsv[i] = make_float2(0.f, 0.f);
     if (live && fl < fpb && f < nfields) {
       const float2 *src = g + (long)f * gs + (long)m * t.nlat;
-      gn = src[lat];
-      if (south != lat) gsv = src[south];
+      gn[i] = __ldg(src + lat);
+      if (south != lat) gsv[i] = __ldg(src + south);
     }
-    const float a = par ? gn.x - gsv.x : gn.x + gsv.x;
-    const float b = par ? gn.y - gsv.y : gn.y + gsv.y;
+  }
+#pragma unroll
+  for (int i = 0; i < NF; i++) {
+    const int fl = warp + 8 * i;
+    const float a = par ? gn[i].x - gsv[i].x : gn[i].x + gsv[i].x;
+    const float b = par ? gn[i].y - gsv[i].y : gn[i].y + gsv[i].y;
     *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl, lane)) = a * w;
     *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl + 1, lane)) = b * w;
   }
