@@ -675,6 +675,8 @@ def main():
         roof["stages"] = {st: {k: v for k, v in stage_roof(st).items()
                                if k in ("bound", "achieved", "unit", "frac")} for st in stages}
         cpu = cpu_baseline(lmax, nlat, nphi, budget_s=10.0, threads=0)
+        one = cpu_baseline(lmax, nlat, nphi, budget_s=5.0, threads=1)
+        cpu["single_thread"] = {k: one[k] for k in ("value", "cores", "sample")}
         line = {
             "metric": METRIC, "value": value, "unit": "SHT pairs/s", "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": ms / K,
@@ -695,6 +697,7 @@ def main():
             "imex": {"model": "schnakenberg (2 species), D1 sweep", "instances": ni,
                      "grid": f"lmax {lmax}, {nlat}x{nphi}", "launches_per_step": imex_launches,
                      "tc_steps_per_s": world * ni * args.imex_steps / (imex_tc_ms / 1e3),
+                     "tc_steps_per_s_per_instance": args.imex_steps / (imex_tc_ms / 1e3),
                      "fp32_steps_per_s": world * ni * max(10, args.imex_steps // 4) / (imex_fp_ms / 1e3),
                      "unit": "instance-steps/s", "finite": ok_tc and ok_fp,
                      "config1": {"workload": "1 Schnakenberg instance, lmax 63, 96x192, "
