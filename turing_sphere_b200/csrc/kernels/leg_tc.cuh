@@ -141,6 +141,25 @@ TS_DEV void ts_tmem_free(unsigned base, unsigned ncols) {
                : "memory");
 }
 
+// An encoded tensor map (the driver's 128-byte CUtensorMap), passed by value
+// as a __grid_constant__ kernel parameter.
+struct __align__(64) TsTmaDesc {
+  unsigned long long v[16];
+};
+
+// 3-D tile store of the shared-memory box at src to element coordinates
+// (x, y, z); completion tracked by the issuing thread's bulk group
+TS_DEV void ts_tma_store3(const TsTmaDesc *map, const void *src, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+          reinterpret_cast<unsigned long long>(map)),
+      "r"(x), "r"(y), "r"(z), "r"(ts_smem_u32(src))
+      : "memory");
+}
+TS_DEV void ts_bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+TS_DEV void ts_bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+TS_DEV void ts_bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // byte offset of element (row r, k) in a K-major 128B-swizzled tile whose
 // rows are 32 tf32 values
 TS_DEV int ts_swz(int r, int k) {
@@ -491,12 +510,16 @@ struct TsSynthSched {
   }
 };
 
-// grid = min(#SMs, tiles), block = 320, persistent.  Dynamic shared memory:
+// grid = min(#SMs, tiles), block = 448, persistent.  Dynamic shared memory:
 // S*(2*16384 + 2*NL*128) + 2*TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe).
-// TMEM: two buffers of 2*NL columns.
+// TMEM: two buffers of 2*NL columns.  With tma_ok, fmap maps fm as floats
+// [field][m][2 nlat] with a (32, 1, 64) box in the 128-byte swizzle, and
+// whole 16-latitude chunks leave through tensor stores (one thread per
+// epilogue group issues them); other chunks, or tma_ok = 0, use plain stores.
 __global__ void __launch_bounds__(TS_TC_THREADS, 1)
 ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb,
-                float2 *__restrict__ fm, long fm_stride, int nfields, int S) {
+                float2 *__restrict__ fm, long fm_stride, int nfields, int S,
+                const __grid_constant__ TsTmaDesc fmap, int tma_ok) {
   extern __shared__ __align__(1024) char ts_smem_st[];
   char *smem = (char *)(((unsigned long long)ts_smem_st + 1023) & ~1023ull);
   const int NL = tc.NL;
@@ -512,11 +535,13 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
   const unsigned tmem = pp->tmem;
 
   // epilogue, per 16 latitudes: each thread (row 2f+re|im) puts north = E+O
-  // and south = E-O of its component into the staging rows; then the 128
-  // threads write 16-byte runs of whole complex values, north in latitude
-  // order and south mirrored, 8 lanes covering one field's 128-byte run
+  // and south = E-O of its component into the group's staging rows; whole
+  // chunks then leave as two tensor stores (north box, mirrored south box),
+  // a partial chunk as 16-byte runs of whole complex values written by the
+  // 128 threads, north in latitude order and south mirrored
   const int grp = ts_epi_group(warp);
   float *sE = reinterpret_cast<float *>(smem + S * stage + (grp > 0 ? TS_TC_SYN_STAGING : 0));
+  const bool elected = warp >= 6 && ((warp - 6) & 3) == 0 && lane == 0;  // one per epilogue group
   const bool vec = (t.nlat % 2 == 0) && (fm_stride % 2 == 0) &&
                    ((reinterpret_cast<unsigned long long>(fm) & 15) == 0);
   auto epilogue = [&](int tile, unsigned tbase) {
@@ -534,6 +559,30 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
       else
 #pragma unroll
         for (int i = 0; i < 16; i++) o[i] = 0.f;
+      // the group's previous tensor stores have read the staging rows
+      if (elected) ts_bulk_wait_read();
+      ts_epi_bar(grp);
+      const int lat0 = lt * NL + c0;
+      if (tma_ok && lat0 + 16 <= t.nh) {
+        // north box [64 fields][16 latitudes x re,im] and south box (its
+        // latitudes mirrored, so in decreasing order of the north ones), both
+        // in the 128-byte swizzle the tensor map writes from
+        char *stN = reinterpret_cast<char *>(sE), *stS = stN + 8192;
+        const int fl = et >> 1, comp = et & 1;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          *reinterpret_cast<float *>(stN + ts_swz(fl, 2 * i + comp)) = e[i] + o[i];
+          *reinterpret_cast<float *>(stS + ts_swz(fl, 2 * (15 - i) + comp)) = e[i] - o[i];
+        }
+        ts_fence_proxy_async();
+        ts_epi_bar(grp);
+        if (elected) {
+          ts_tma_store3(&fmap, stN, 2 * lat0, m, fb * TS_TC_FIELDS);
+          ts_tma_store3(&fmap, stS, 2 * (t.nlat - lat0 - 16), m, fb * TS_TC_FIELDS);
+          ts_bulk_commit();
+        }
+        continue;
+      }
 #pragma unroll
       for (int i = 0; i < 16; i++) {
         mine[2 * i] = e[i] + o[i];
@@ -572,6 +621,7 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
     }
   };
   ts_tc_persistent(smem, pp, S, stage, tmem, 2 * NL, sc, epilogue);
+  if (elected) ts_bulk_wait_all();
   ts_tc_fence_before();
   __syncthreads();
   if (pp->bad && tid == 0) atomicExch(tc.err, 1);

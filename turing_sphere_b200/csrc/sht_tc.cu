@@ -1,5 +1,9 @@
 // Tensor-core Legendre tables (FP64 on the GPU) and launchers.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
+#include <cstring>
 #include <cstdlib>
 #include <vector>
 
@@ -357,14 +361,47 @@ void ts_launch_wimage(ts_plan p, const float2 *g, long gs, int nf, int fpb, char
   TS_CUDA(cudaGetLastError());
 }
 
+static_assert(sizeof(TsTmaDesc) == sizeof(CUtensorMap), "tensor map size");
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// fm[field][m][lat] (float2, field stride fs) as floats [field][m][2 nlat],
+// box (16 latitudes x re,im = 32 floats, 1 m, 64 fields), 128-byte swizzle
+bool fm_store_map(ts_plan p, TsTmaDesc *map, float2 *fm, long fs, int nf) {
+  const auto encode = tma_encoder();
+  if (!encode || (reinterpret_cast<uintptr_t>(fm) & 15) || (p->nlat & 1) || (fs & 1)) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * p->nlat, (cuuint64_t)p->mmax + 1, (cuuint64_t)nf};
+  const cuuint64_t strides[2] = {(cuuint64_t)p->nlat * 8, (cuuint64_t)fs * 8};
+  const cuuint32_t box[3] = {32, 1, TS_TC_FIELDS};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return encode(reinterpret_cast<CUtensorMap *>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, fm, dims,
+                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+}  // namespace
+
 void ts_launch_synth_tc_img(ts_plan p, const char *qimg, int nf, float2 *fm, long fs,
                             cudaStream_t s) {
+  TsTmaDesc map;
+  memset(&map, 0, sizeof map);
+  const int tma_ok = fm_store_map(p, &map, fm, fs, nf) ? 1 : 0;  // else plain stores
   ts_allow_smem((const void *)ts_leg_synth_tc, p->ctx->device, ts_tc_synth_smem(p));
   const TsTcTab &tc = ts_tc_tab(p);
   const int nfb = (nf + TS_TC_FIELDS - 1) / TS_TC_FIELDS;
   const int ctas = ts_tc_ctas(p, (long)(p->mmax + 1) * tc.nLT * nfb);
   ts_leg_synth_tc<<<ctas, TS_TC_THREADS, ts_tc_synth_smem(p), s>>>(p->leg, tc, qimg, nfb, fm, fs,
-                                                                   nf, synth_stages(p));
+                                                                   nf, synth_stages(p), map, tma_ok);
   TS_CUDA(cudaGetLastError());
 }
 
