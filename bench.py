@@ -179,6 +179,40 @@ def cpu_baseline(lmax, nlat, nphi, budget_s=10.0, threads=0):
                       f"summation (oracle restating src/sht/reference.ts), {dt:.1f} s"}
 
 
+def cpu_baselines_extra():
+    """The rest of the CPU baseline plan: SHT pairs/s at lmax 127 and 511 on
+    one core and on all cores (bounded samples: 1-3 pairs at lmax 511), and
+    Schnakenberg IMEX steps/s at lmax 63 (96x192) on one core, all by the f64
+    oracle on the host."""
+    from oracle import oracle as O
+    out = {}
+    for lm, budget in ((127, 2.0), (511, 3.0)):
+        nlat, nphi = grid(lm)
+        row = {}
+        for key, th in (("all_cores", 0), ("single_thread", 1)):
+            r = cpu_baseline(lm, nlat, nphi, budget_s=budget, threads=th)
+            row[key] = {"value": r["value"], "cores": r["cores"], "sample": r["sample"]}
+        out[f"sht_pairs_lmax{lm}"] = row
+    ref = O.ShtReference(63, 63, 96, 192, threads=1)
+    p = {"a": 0.1, "b": 0.9, "D1": 4e-4, "D2": 8e-3, "dt": 0.05}
+    u00 = (p["a"] + p["b"]) * math.sqrt(4 * math.pi)
+    st = np.zeros((2, 2 * ref.nlm))
+    st[0, 0] = u00
+    st[1, 0] = p["b"] / (p["a"] + p["b"]) ** 2 * math.sqrt(4 * math.pi)
+    st += 1e-3 * np.random.default_rng(1).standard_normal(st.shape)
+    prm = [p["a"], p["b"], p["D1"], p["D2"], p["dt"]]
+    ref.model_step("schnakenberg", prm, st, 2)
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < 3.0:
+        st = ref.model_step("schnakenberg", prm, st, 20)
+        n += 20
+    dt = time.perf_counter() - t0
+    out["imex_schnakenberg_lmax63"] = {
+        "value": n / dt, "unit": "steps/s", "cores": 1,
+        "sample": f"{n} IMEX steps of one instance at lmax 63 (96x192), f64 oracle, {dt:.1f} s"}
+    return out
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU transform path, restated (oracle)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -677,6 +711,7 @@ def main():
         cpu = cpu_baseline(lmax, nlat, nphi, budget_s=10.0, threads=0)
         one = cpu_baseline(lmax, nlat, nphi, budget_s=5.0, threads=1)
         cpu["single_thread"] = {k: one[k] for k in ("value", "cores", "sample")}
+        cpu["other_configs"] = cpu_baselines_extra()
         line = {
             "metric": METRIC, "value": value, "unit": "SHT pairs/s", "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": ms / K,
