@@ -453,7 +453,12 @@ TS_DEV void ts_f2_write_w(const float2 *b, int lat0, long f, const TsFftTab &ft,
   const int o_re = ts_swz_img(2 * fl, lat & 31), o_im = ts_swz_img(2 * fl + 1, lat & 31);
   char *base = wimg + ((long)fb * 2 * nlc + (lat >> 5)) * 16384;
   const long kstep = (long)nfb * 2 * nlc * 16384, pstep = (long)nlc * 16384;
-  for (int k = threadIdx.x / NPR; k <= ft.mmax; k += 2 * C::P) {
+  // k groups g = threadIdx.x / NPR (2P of them), permuted so that the two
+  // halves of a half-warp take k 8 apart: their row reads then fall in
+  // disjoint banks (a bijection when 2P is a multiple of 16)
+  const int g = threadIdx.x / NPR;
+  const int k0 = (2 * C::P) % 16 == 0 ? (g & ~15) + ((g & 1) << 3) + ((g >> 1) & 7) : g;
+  for (int k = k0; k <= ft.mmax; k += 2 * C::P) {
     const float2 xn = ts_f2_xk<C>(rn, k, ft);
     const float2 xs = south ? ts_f2_xk<C>(rs, k, ft) : make_float2(0.f, 0.f);
     char *blk = base + k * kstep;
