@@ -163,6 +163,22 @@ struct TsF2 {
   static constexpr int TWQ = Q_ * P1;      // inter-phase twiddles [n2][k1]
 };
 
+// Thread -> (row r, k1) of the phases that run one Q-point DFT per (r, k1).
+// With R >= 16 rows a half-warp takes one k1 of 16 consecutive rows: the odd
+// row pitch spreads them over 16 distinct banks and they share one twiddle
+// (rows first would put two rows in some half-warps, whose columns k1 and
+// k1 + 16 collide); with fewer rows the rows stay together.
+template <class C>
+TS_DEV void ts_f2_rk(int tid, int &r, int &k1) {
+  if constexpr (C::R >= 16) {
+    k1 = tid / C::R;
+    r = tid - k1 * C::R;
+  } else {
+    r = tid / C::P;
+    k1 = tid - r * C::P;
+  }
+}
+
 // twq[n2 (P+1) + k1] = w^{n2 k1}
 template <class C>
 TS_DEV void ts_f2_twq(float2 *twq, const TsFftTab &ft) {
@@ -177,7 +193,8 @@ template <class C>
 TS_DEV void ts_f2_inverse(float2 *b, const float2 *twq) {
   const int tid = threadIdx.x;
   {
-    const int r = tid / C::P, k1 = tid - r * C::P;
+    int r, k1;
+  ts_f2_rk<C>(tid, r, k1);
     float2 *row = b + r * C::RP;
     float2 x[C::Q];
 #pragma unroll
@@ -233,7 +250,8 @@ TS_DEV void ts_f2_forward(float2 *b, const float2 *twq) {
     __syncthreads();
   }
   {
-    const int r = tid / C::P, k1 = tid - r * C::P;
+    int r, k1;
+  ts_f2_rk<C>(tid, r, k1);
     float2 *row = b + r * C::RP;
     float2 x[C::Q];
 #pragma unroll
@@ -254,7 +272,8 @@ TS_DEV void ts_f2_inverse_out(float2 *b, const float2 *twq, float *__restrict__ 
                               LatOf lat_of) {
   const int tid = threadIdx.x;
   {
-    const int r = tid / C::P, k1 = tid - r * C::P;
+    int r, k1;
+  ts_f2_rk<C>(tid, r, k1);
     float2 *row = b + r * C::RP;
     float2 x[C::Q];
 #pragma unroll
@@ -309,7 +328,8 @@ TS_DEV void ts_f2_forward_in(float2 *b, const float2 *twq, const float *__restri
   }
   __syncthreads();
   {
-    const int r = tid / C::P, k1 = tid - r * C::P;
+    int r, k1;
+  ts_f2_rk<C>(tid, r, k1);
     float2 *row = b + r * C::RP;
     float2 x[C::Q];
 #pragma unroll
@@ -576,7 +596,8 @@ ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
 template <class C>
 TS_DEV void ts_f2_inv_phase1(float2 *b, const float2 *twq) {
   const int tid = threadIdx.x;
-  const int r = tid / C::P, k1 = tid - r * C::P;
+  int r, k1;
+  ts_f2_rk<C>(tid, r, k1);
   float2 *row = b + r * C::RP;
   float2 x[C::Q];
 #pragma unroll
@@ -595,7 +616,8 @@ TS_DEV void ts_f2_inv_phase1(float2 *b, const float2 *twq) {
 template <class C>
 TS_DEV void ts_f2_fwd_phase2(float2 *b) {
   const int tid = threadIdx.x;
-  const int r = tid / C::P, k1 = tid - r * C::P;
+  int r, k1;
+  ts_f2_rk<C>(tid, r, k1);
   float2 *row = b + r * C::RP;
   float2 x[C::Q];
 #pragma unroll
