@@ -111,6 +111,11 @@ typedef struct ts_plan_info {
   int fft_p, fft_q;  /* two-phase FFT H = P*Q (0 when the Stockham/DFT kernels run) */
   int fft_rows;      /* grid rows per FFT CTA */
   int tuned;         /* 1 when the shapes were timed (TS_PLAN_AUTOTUNE) */
+  /* tensor-core polar skip: synthesis tiles written as zeros, and synthesis
+   * degree chunks plus analysis latitude chunks left out, because every
+   * table value in them is below 1e-10 of the largest of their m (synthesis)
+   * or tile (analysis) */
+  int tc_skip_tiles, tc_skip_chunks;
 } ts_plan_info;
 int ts_sht_plan_info(ts_plan plan, ts_plan_info *info);
 

@@ -157,3 +157,26 @@ def test_bounded_waits_time_out_and_the_plan_recovers(device):
     fp32 = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi), {"precision": "fp32"})
     with pytest.raises(TsError):
         fp32.testStall(True)
+
+
+@pytest.mark.parametrize("lmax,nlat,nphi", [(255, 384, 768), (511, 768, 1536)])
+def test_polar_skip_drops_work_not_accuracy(device, lmax, nlat, nphi):
+    """The polar skip leaves out synthesis tiles and analysis latitude chunks
+    whose table values are all below 1e-10 of their m's (tile's) largest; the
+    high-m coefficients, the only ones it touches, stay within tolerance of
+    the f64 oracle in both directions."""
+    plan = tc_plan(device, lmax, nlat, nphi)
+    assert plan.shapes["tc_skip_tiles"] > 0 and plan.shapes["tc_skip_chunks"] > 0
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = scaled_spectrum(lmax, lmax, 31)
+    high = np.zeros_like(q)
+    m0 = lmax // 2
+    start = 2 * (m0 * (lmax + 1) - m0 * (m0 - 1) // 2)  # first coefficient of m = m0
+    high[start:] = q[start:]
+    s64 = ref.synth(high.astype(np.float64))
+    assert O.rel_l2(plan.synth(high), s64) < TOL
+    s32 = s64.astype(np.float32)
+    q64 = ref.analys(s32.astype(np.float64))
+    qa = plan.analys(s32)
+    assert O.rel_l2(qa[start:], q64[start:]) < TOL
+    plan.status()

@@ -54,6 +54,7 @@ class PlanInfo(C.Structure):
         ("fft_stages", C.c_int), ("fft_radix", C.c_int * 16), ("table_bytes", C.c_long),
         ("tc_lat_tile", C.c_int), ("tc_deg_tile", C.c_int), ("fft_p", C.c_int),
         ("fft_q", C.c_int), ("fft_rows", C.c_int), ("tuned", C.c_int),
+        ("tc_skip_tiles", C.c_int), ("tc_skip_chunks", C.c_int),
     ]
 
 

@@ -310,6 +310,7 @@ int ts_sht_plan_info(ts_plan p, ts_plan_info *info) {
     const TsTcGeom g = ts_tc_geom(p);
     info->tc_lat_tile = g.NL;
     info->tc_deg_tile = g.LTL;
+    ts_tc_skip_counts(p, &info->tc_skip_tiles, &info->tc_skip_chunks);
   }
   int P = 0, Q = 0;
   if (ts_f2_shape(p, &P, &Q)) {

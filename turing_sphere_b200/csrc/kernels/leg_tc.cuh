@@ -473,25 +473,30 @@ struct TsSynthSched {
       cc = (t_ - both) + min(n0, n1);
     }
   }
+  // leading (parity 0, parity 1) degree-chunk pairs of tile (m, lt) whose
+  // table values are all negligible (the polar skip); the stage index t_ of
+  // the remaining stages maps to t_ + 2 cs in the full sequence
+  TS_DEV int cs(int m, int lt) const { return tc->syn_cs ? tc->syn_cs[m * nLT + lt] : 0; }
   TS_DEV int stages(int tile) const {
     int m, lt, fb, n0, n1;
     decode(tile, m, lt, fb);
+    if (tc->syn_zero && tc->syn_zero[m * nLT + lt]) return 0;  // polar tile: zeros
     nch(m, n0, n1);
-    return n0 + n1;
+    return n0 + n1 - 2 * cs(m, lt);
   }
   TS_DEV unsigned table_bytes(int) const { return 2u * NL * 128; }
   TS_DEV int n(int) const { return NL; }
   TS_DEV const char *a_src(int tile, int t_) const {
     int m, lt, fb, par, cc, n0, n1;
     decode(tile, m, lt, fb);
-    parcc(m, t_, par, cc);
+    parcc(m, t_ + 2 * cs(m, lt), par, cc);
     nch(m, n0, n1);
     return qimg + ((long)(tc->chunk_prefix[m] + (par ? n0 : 0) + cc) * nfb + fb) * 16384;
   }
   TS_DEV const char *b_src(int tile, int t_) const {
     int m, lt, fb, par, cc, n0, n1;
     decode(tile, m, lt, fb);
-    parcc(m, t_, par, cc);
+    parcc(m, t_ + 2 * cs(m, lt), par, cc);
     nch(m, n0, n1);
     const long bb = 2L * NL * 128;
     return tc->synth + tc->synth_off[m] + (long)((par ? n0 : 0) + cc) * nLT * bb + (long)lt * bb;
@@ -499,14 +504,15 @@ struct TsSynthSched {
   TS_DEV int d_col(int tile, int t_) const {
     int m, lt, fb, par, cc;
     decode(tile, m, lt, fb);
-    parcc(m, t_, par, cc);
+    parcc(m, t_ + 2 * cs(m, lt), par, cc);
     return par * NL;
   }
   TS_DEV bool first(int tile, int t_) const {
     int m, lt, fb, par, cc;
     decode(tile, m, lt, fb);
-    parcc(m, t_, par, cc);
-    return cc == 0;
+    const int c = cs(m, lt);
+    parcc(m, t_ + 2 * c, par, cc);
+    return cc == c;
   }
 };
 
@@ -551,14 +557,20 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
     const int et = ts_epi_row(warp, lane);  // 0..127 = TMEM lane = 2*field + comp
     float *mine = sE + (et >> 1) * TS_TC_SYN_ROW + (et & 1);
     const unsigned lanebase = tbase + ((unsigned)((warp & 3) * 32) << 16);
+    const bool zero = sc.stages(tile) == 0;  // a polar tile: no MMAs ran
     for (int c0 = 16 * grp; c0 < NL; c0 += 32) {
       float e[16], o[16];
-      ts_tmem_ld16(lanebase + (unsigned)c0, e);
-      if (n1 > 0)
-        ts_tmem_ld16(lanebase + (unsigned)(NL + c0), o);
-      else
+      if (zero) {
 #pragma unroll
-        for (int i = 0; i < 16; i++) o[i] = 0.f;
+        for (int i = 0; i < 16; i++) e[i] = o[i] = 0.f;
+      } else {
+        ts_tmem_ld16(lanebase + (unsigned)c0, e);
+        if (n1 > 0)
+          ts_tmem_ld16(lanebase + (unsigned)(NL + c0), o);
+        else
+#pragma unroll
+          for (int i = 0; i < 16; i++) o[i] = 0.f;
+      }
       // the group's previous tensor stores have read the staging rows
       if (elected) ts_bulk_wait_read();
       ts_epi_bar(grp);
@@ -647,18 +659,26 @@ struct TsAnalysSched {
     decode(tile, m, par, lt, fb);
     return ts_atile_count(lmax, m, par, lt, tc->LTL);
   }
-  TS_DEV int stages(int tile) const { return cnt(tile) > 0 ? tc->nLC : 0; }
+  // leading latitude chunks skipped (their table values are all negligible)
+  TS_DEV int c0(int tile) const {
+    if (!tc->ana_c0) return 0;
+    int m, par, lt, fb;
+    decode(tile, m, par, lt, fb);
+    return tc->ana_c0[(2 * m + par) * tc->ntile + lt];
+  }
+  TS_DEV int stages(int tile) const { return cnt(tile) > 0 ? tc->nLC - c0(tile) : 0; }
   TS_DEV int n(int tile) const { return max(16, ts_round16(cnt(tile))); }
   TS_DEV unsigned table_bytes(int tile) const { return 2u * n(tile) * 128; }
   TS_DEV const char *a_src(int tile, int c) const {
     int m, par, lt, fb;
     decode(tile, m, par, lt, fb);
-    return wimg + ((((long)m * nfb + fb) * 2 + par) * tc->nLC + c) * 16384;
+    return wimg + ((((long)m * nfb + fb) * 2 + par) * tc->nLC + c + c0(tile)) * 16384;
   }
   TS_DEV const char *b_src(int tile, int c) const {
     int m, par, lt, fb;
     decode(tile, m, par, lt, fb);
-    return tc->anal + ts_atile_offset(*tc, lmax, m, par, lt) + (long)c * table_bytes(tile);
+    return tc->anal + ts_atile_offset(*tc, lmax, m, par, lt) +
+           (long)(c + c0(tile)) * table_bytes(tile);
   }
   TS_DEV int d_col(int, int) const { return 0; }
   TS_DEV bool first(int, int c) const { return c == 0; }
@@ -693,6 +713,7 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
   auto epilogue = [&](int tile, unsigned tbase) {
     const int cnt = sc.cnt(tile);
     if (cnt == 0) return;
+    const bool zero = sc.stages(tile) == 0;  // every chunk skipped: no MMAs ran
     int m, par, lt, fb;
     sc.decode(tile, m, par, lt, fb);
     const int N = ts_round16(cnt);
@@ -706,7 +727,12 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
       ts_epi_bar(grp);  // the previous epi calls are done with sD
       for (int c0 = 0; c0 < hn; c0 += 16) {
         float v[16];
-        ts_tmem_ld16(lanebase + (unsigned)(h0 + c0), v);
+        if (zero) {
+#pragma unroll
+          for (int i = 0; i < 16; i++) v[i] = 0.f;
+        } else {
+          ts_tmem_ld16(lanebase + (unsigned)(h0 + c0), v);
+        }
 #pragma unroll
         for (int i = 0; i < 16; i++) sD[((c0 + i) * 2 + comp) * TS_TC_ANA_ROW + fl] = v[i];
       }

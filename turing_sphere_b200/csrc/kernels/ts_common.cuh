@@ -120,6 +120,14 @@ struct TsTcTab {
   int nchunks;
   unsigned wait_limit;      // polls before a bounded wait gives up (0: the default)
   int stall_copies;         // test hook: the copy warp issues nothing, every wait runs out
+  // Polar skip (null: none).  syn_zero[m nLT + lt] = 1 when every table value
+  // of synthesis tile (m, lt) is below the skip threshold (the tile's output
+  // is written as zeros); ana_c0[(2 m + par) ntile + ltile] = leading latitude
+  // chunks of an analysis tile whose table values are all below it (skipped).
+  const unsigned char *syn_zero;
+  const unsigned char *syn_cs;  // leading degree-chunk pairs of tile (m, lt) left out
+  const int *ana_c0;
+  int ntile;
 };
 
 // The data operands of the tensor-core Legendre stage, kept in HBM as raw fp32

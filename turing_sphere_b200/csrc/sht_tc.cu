@@ -121,16 +121,174 @@ TsTcGeom ts_tc_geom(ts_plan p) {
   return g;
 }
 
+// max |value| over the first n[b] floats at img + off[b] (the hi halves of
+// table blocks); one CTA per block
+__global__ void ts_k_block_absmax(const char *img, const long *off, const int *n, int nb,
+                                  float *out) {
+  __shared__ float red[8];
+  const int b = blockIdx.x;
+  if (b >= nb) return;
+  const float *v = reinterpret_cast<const float *>(img + off[b]);
+  float mx = 0.f;
+  for (int i = threadIdx.x; i < n[b]; i += blockDim.x) mx = fmaxf(mx, fabsf(v[i]));
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) mx = fmaxf(mx, red[w]);
+    out[b] = fmaxf(red[0], mx);
+  }
+}
+
+// Relative size below which a table value is dropped by the polar skip: the
+// dropped terms are then ~10^3 below the FP32 rounding of the kept ones.
+constexpr double kPolarSkip = 1e-10;
+
 struct ts_tc_tables {
   char *synth = nullptr, *anal = nullptr;
   long *synth_off = nullptr, *anal_off = nullptr;
   int *err = nullptr;
   int *chunk_prefix = nullptr, *chunk_m = nullptr, *chunk_pc = nullptr;
+  unsigned char *syn_zero = nullptr, *syn_cs = nullptr;
+  int *ana_c0 = nullptr;
+  // synthesis tiles, synthesis degree chunks and analysis latitude chunks the polar skip drops
+  int skip_syn = 0, skip_syn_chunks = 0, skip_ana = 0;
   ts_dbuf qimg, wimg, gscratch;  // operand images and a G scratch of the standalone transforms
   TsTcTab tab{};
   size_t bytes = 0;
   int ntile = 1;  // analysis l tiles per parity (grid.z = 2*ntile)
 };
+
+// Polar skip (the associated Legendre functions of high m vanish to many
+// digits near the poles): find the synthesis tiles and the leading analysis
+// latitude chunks whose table values are all below kPolarSkip times the
+// largest value of their m (synthesis) or of their tile (analysis), from the
+// tables themselves, and give the kernels the skip lists.
+void tc_polar_skip(ts_plan p, ts_tc_tables *t, const std::vector<long> &soff,
+                   const std::vector<long> &aoff, int nLC) {
+  if (const char *e = getenv("TS_TC_POLAR_SKIP"))
+    if (e[0] == '0') return;
+  const TsTcGeom gm = ts_tc_geom(p);
+  const int NL = gm.NL, nLT = gm.nLT, LTL = gm.LTL, M = p->mmax + 1;
+  // synthesis blocks (m, chunk, lt): hi half = NL rows x 32 floats
+  std::vector<long> off;
+  std::vector<int> n;
+  std::vector<int> sblk_m, sblk_lt;
+  for (int m = 0; m < M; m++) {
+    int nch = 0;
+    for (int par = 0; par < 2; par++) nch += (kpar_h(p->lmax, m, par) + TS_TC_KCH - 1) / TS_TC_KCH;
+    for (int ch = 0; ch < nch; ch++)
+      for (int lt = 0; lt < nLT; lt++) {
+        off.push_back(soff[m] + ((long)ch * nLT + lt) * 2 * NL * 128);
+        n.push_back(NL * 32);
+        sblk_m.push_back(m);
+        sblk_lt.push_back(lt);
+      }
+  }
+  const size_t nsyn = off.size();
+  // analysis blocks (m, par, ltile, c): hi half = N rows x 32 floats
+  std::vector<int> ablk_tile;  // (2 m + par) ntile + ltile
+  for (int m = 0; m < M; m++) {
+    long a = aoff[m];
+    for (int par = 0; par < 2; par++) {
+      const int kp = kpar_h(p->lmax, m, par);
+      for (int lt = 0, lo = 0; lo < kp; lt++, lo += LTL) {
+        const int N = ((std::min(kp, lo + LTL) - lo + 15) / 16) * 16;
+        for (int c = 0; c < nLC; c++) {
+          off.push_back(a + (long)c * 2 * N * 128);
+          n.push_back(N * 32);
+          ablk_tile.push_back((2 * m + par) * t->ntile + lt);
+        }
+        a += (long)nLC * 2 * N * 128;
+      }
+    }
+  }
+  const size_t nb = off.size();
+  long *d_off = nullptr;
+  int *d_n = nullptr;
+  float *d_mx = nullptr;
+  TS_CUDA(cudaMalloc(&d_off, sizeof(long) * nb));
+  TS_CUDA(cudaMalloc(&d_n, sizeof(int) * nb));
+  TS_CUDA(cudaMalloc(&d_mx, sizeof(float) * nb));
+  TS_CUDA(cudaMemcpy(d_off, off.data(), sizeof(long) * nb, cudaMemcpyHostToDevice));
+  TS_CUDA(cudaMemcpy(d_n, n.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+  if (nsyn)
+    ts_k_block_absmax<<<(unsigned)nsyn, 256, 0, p->ctx->stream>>>(t->synth, d_off, d_n, (int)nsyn,
+                                                                  d_mx);
+  if (nb > nsyn)
+    ts_k_block_absmax<<<(unsigned)(nb - nsyn), 256, 0, p->ctx->stream>>>(
+        t->anal, d_off + nsyn, d_n + nsyn, (int)(nb - nsyn), d_mx + nsyn);
+  std::vector<float> mx(nb);
+  TS_CUDA(cudaGetLastError());
+  TS_CUDA(cudaMemcpyAsync(mx.data(), d_mx, sizeof(float) * nb, cudaMemcpyDeviceToHost,
+                          p->ctx->stream));
+  TS_CUDA(cudaStreamSynchronize(p->ctx->stream));
+  cudaFree(d_off);
+  cudaFree(d_n);
+  cudaFree(d_mx);
+  // synthesis: tile (m, lt) is dropped when all its blocks are negligible
+  std::vector<double> mmax_m(M, 0.0), tmax(M * nLT, 0.0);
+  for (size_t b = 0; b < nsyn; b++) {
+    mmax_m[sblk_m[b]] = std::max(mmax_m[sblk_m[b]], (double)mx[b]);
+    double &tm = tmax[sblk_m[b] * nLT + sblk_lt[b]];
+    tm = std::max(tm, (double)mx[b]);
+  }
+  // leading degree-chunk pairs of each tile, both parities negligible; at
+  // least one chunk of each parity stays (it initialises the accumulator)
+  std::vector<unsigned char> csk(M * nLT, 0);
+  {
+    size_t b = 0;
+    for (int m = 0; m < M; m++) {
+      const int n0 = (kpar_h(p->lmax, m, 0) + TS_TC_KCH - 1) / TS_TC_KCH;
+      const int n1 = (kpar_h(p->lmax, m, 1) + TS_TC_KCH - 1) / TS_TC_KCH;
+      const size_t mb = b;  // block (ch, lt) of m at mb + ch nLT + lt
+      b += (size_t)(n0 + n1) * nLT;
+      if (n1 == 0) continue;
+      const int cap = std::min(std::min(n0, n1) - 1, 255);
+      for (int lt = 0; lt < nLT; lt++) {
+        int c = 0;
+        while (c < cap && mx[mb + (size_t)c * nLT + lt] < kPolarSkip * mmax_m[m] &&
+               mx[mb + (size_t)(n0 + c) * nLT + lt] < kPolarSkip * mmax_m[m])
+          c++;
+        csk[m * nLT + lt] = (unsigned char)c;
+      }
+    }
+  }
+  std::vector<unsigned char> zero(M * nLT, 0);
+  for (int m = 0; m < M; m++)
+    for (int lt = 0; lt < nLT; lt++)
+      if (mmax_m[m] > 0 && tmax[m * nLT + lt] < kPolarSkip * mmax_m[m]) {
+        zero[m * nLT + lt] = 1;
+        t->skip_syn++;
+      }
+  // analysis: leading chunks of a tile below the threshold of the tile's max
+  const int ntiles = 2 * M * t->ntile;
+  std::vector<double> amax(ntiles, 0.0);
+  for (size_t b = nsyn; b < nb; b++)
+    amax[ablk_tile[b - nsyn]] = std::max(amax[ablk_tile[b - nsyn]], (double)mx[b]);
+  std::vector<int> c0(ntiles, 0);
+  std::vector<int> seen(ntiles, 0);
+  for (size_t b = nsyn; b < nb; b++) {  // blocks of a tile come in chunk order
+    const int tl = ablk_tile[b - nsyn];
+    if (seen[tl]) continue;
+    if (mx[b] < kPolarSkip * amax[tl])
+      c0[tl]++;
+    else
+      seen[tl] = 1;
+  }
+  for (int tl = 0; tl < ntiles; tl++) t->skip_ana += c0[tl];
+  for (int i = 0; i < M * nLT; i++)
+    if (!zero[i]) t->skip_syn_chunks += 2 * csk[i];
+  TS_CUDA(cudaMalloc(&t->syn_cs, csk.size()));
+  TS_CUDA(cudaMemcpy(t->syn_cs, csk.data(), csk.size(), cudaMemcpyHostToDevice));
+  t->tab.syn_cs = t->syn_cs;
+  TS_CUDA(cudaMalloc(&t->syn_zero, zero.size()));
+  TS_CUDA(cudaMalloc(&t->ana_c0, sizeof(int) * c0.size()));
+  TS_CUDA(cudaMemcpy(t->syn_zero, zero.data(), zero.size(), cudaMemcpyHostToDevice));
+  TS_CUDA(cudaMemcpy(t->ana_c0, c0.data(), sizeof(int) * c0.size(), cudaMemcpyHostToDevice));
+  t->tab.syn_zero = t->syn_zero;
+  t->tab.ana_c0 = t->ana_c0;
+}
 
 void ts_tc_init(ts_plan p) {
   auto *t = new ts_tc_tables();
@@ -197,18 +355,24 @@ void ts_tc_init(ts_plan p) {
   tc.chunk_m = t->chunk_m;
   tc.chunk_pc = t->chunk_pc;
   tc.nchunks = (int)cm.size();
+  tc.ntile = t->ntile;
+  tc.syn_zero = nullptr;
+  tc.syn_cs = nullptr;
+  tc.ana_c0 = nullptr;
   dim3 grid((nh + 63) / 64, p->mmax + 1);
   ts_k_tc_tables<<<grid, 64, 0, p->ctx->stream>>>(p->lmax, p->mmax, nh, p->d_x64, p->d_ab64,
                                                   p->d_amm64, tc, t->synth, t->anal);
   TS_CUDA(cudaGetLastError());
   TS_CUDA(cudaStreamSynchronize(p->ctx->stream));
+  tc_polar_skip(p, t, soff, aoff, nLC);
 }
 
 void ts_tc_free(ts_plan p) {
   auto *t = static_cast<ts_tc_tables *>(p->tc);
   if (!t) return;
   for (void *q : {(void *)t->synth, (void *)t->anal, (void *)t->synth_off, (void *)t->anal_off,
-                  (void *)t->err, (void *)t->chunk_prefix, (void *)t->chunk_m, (void *)t->chunk_pc})
+                  (void *)t->err, (void *)t->chunk_prefix, (void *)t->chunk_m, (void *)t->chunk_pc,
+                  (void *)t->syn_zero, (void *)t->syn_cs, (void *)t->ana_c0})
     if (q) cudaFree(q);
   t->qimg.release();
   t->wimg.release();
@@ -223,6 +387,11 @@ void ts_tc_set_fault(ts_plan p, int stall_copies, unsigned wait_limit) {
   TsTcTab &t = static_cast<ts_tc_tables *>(p->tc)->tab;
   t.stall_copies = stall_copies;
   t.wait_limit = wait_limit;
+}
+void ts_tc_skip_counts(ts_plan p, int *tiles, int *chunks) {
+  const auto *t = static_cast<ts_tc_tables *>(p->tc);
+  *tiles = t ? t->skip_syn : 0;
+  *chunks = t ? t->skip_ana + t->skip_syn_chunks : 0;
 }
 int ts_tc_ntile(ts_plan p) { return static_cast<ts_tc_tables *>(p->tc)->ntile; }
 size_t ts_tc_bytes(ts_plan p) { return p->tc ? static_cast<ts_tc_tables *>(p->tc)->bytes : 0; }

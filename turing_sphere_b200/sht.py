@@ -86,7 +86,8 @@ class ShtPlan:
         # kernel shapes in use: tensor-core tiles, two-phase FFT split, FFT rows per CTA
         self.shapes = {"tc_lat_tile": info.tc_lat_tile, "tc_deg_tile": info.tc_deg_tile,
                        "fft_p": info.fft_p, "fft_q": info.fft_q, "fft_rows": info.fft_rows,
-                       "tuned": bool(info.tuned)}
+                       "tuned": bool(info.tuned), "tc_skip_tiles": info.tc_skip_tiles,
+                       "tc_skip_chunks": info.tc_skip_chunks}
         x = np.zeros(cfg.nlat)
         w = np.zeros(cfg.nlat)
         _lib.check(_lib.lib().ts_sht_plan_nodes(handle, _lib.dptr(x), _lib.dptr(w)), device.handle)
