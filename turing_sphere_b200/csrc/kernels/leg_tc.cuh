@@ -328,9 +328,10 @@ TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes
       return;
     }
     ts_tc_fence_after();
-    const int T = sc.stages(tile);
-    const unsigned tb = sc.table_bytes(tile);
-    const unsigned idesc = ts_idesc_tf32(sc.n(tile));
+    const auto ti = sc.tile(tile);
+    const int T = sc.stages(ti);
+    const unsigned tb = sc.table_bytes(ti);
+    const unsigned idesc = ts_idesc_tf32(sc.n(ti));
     for (int t_ = 0; t_ < T; t_++, g++) {
       const int s = (int)(g % S);
       const unsigned use = (unsigned)(g / S);
@@ -341,8 +342,8 @@ TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes
       ts_tc_fence_after();
       const unsigned ahi = ts_smem_u32(smem + s * stage_bytes), alo = ahi + 16384;
       const unsigned bhi = ahi + 2 * 16384, blo = bhi + tb / 2;
-      const unsigned d = tmem + (unsigned)(b * acc_cols + sc.d_col(tile, t_));
-      const bool init = sc.first(tile, t_);
+      const unsigned d = tmem + (unsigned)(b * acc_cols + sc.d_col(ti, t_));
+      const bool init = sc.first(ti, t_);
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) {
         const unsigned acc = (!init || kk > 0) ? 1u : 0u;
@@ -389,8 +390,9 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
     if (lane == 0 && !sc.tc->stall_copies) {
       long g = 0;
       for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x) {
-        const int T = sc.stages(tile);
-        const unsigned tb = sc.table_bytes(tile);
+        const auto ti = sc.tile(tile);
+        const int T = sc.stages(ti);
+        const unsigned tb = sc.table_bytes(ti);
         int t_ = 0;
         for (; t_ < T; t_++, g++) {
           const int s = (int)(g % S);
@@ -401,8 +403,8 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
           }
           char *st = smem + s * stage_bytes;
           ts_mbar_arrive_tx(&pp->full[s], 16384 + tb);
-          ts_bulk_g2s(st, sc.a_src(tile, t_), 16384, &pp->full[s]);
-          ts_bulk_g2s(st + 2 * 16384, sc.b_src(tile, t_), tb, &pp->full[s]);
+          ts_bulk_g2s(st, sc.a_src(ti, t_), 16384, &pp->full[s]);
+          ts_bulk_g2s(st + 2 * 16384, sc.b_src(ti, t_), tb, &pp->full[s]);
         }
         if (t_ < T) break;
       }
@@ -450,6 +452,14 @@ struct TsSynthSched {
   const TsTcTab *tc;
   int lmax, mmax, nfb, NL, nLT;
   const char *qimg;
+  // what the roles need of one tile, computed once per tile
+  struct Tile {
+    int n0, n1;   // degree chunks of parity 0 / 1
+    int cs;       // leading chunk pairs left out by the polar skip
+    int T;        // stages that run
+    const char *q;  // Q image block of (chunk 0 of m, field block)
+    const char *b;  // table block of (chunk 0 of m, latitude tile)
+  };
   TS_DEV int ntiles() const { return (mmax + 1) * nLT * nfb; }
   TS_DEV void decode(int tile, int &m, int &lt, int &fb) const {
     m = tile / (nLT * nfb);
@@ -461,58 +471,53 @@ struct TsSynthSched {
     n0 = (ts_kpar(lmax, m, 0) + TS_TC_KCH - 1) / TS_TC_KCH;
     n1 = (ts_kpar(lmax, m, 1) + TS_TC_KCH - 1) / TS_TC_KCH;
   }
-  TS_DEV void parcc(int m, int t_, int &par, int &cc) const {
-    int n0, n1;
-    nch(m, n0, n1);
-    const int both = 2 * min(n0, n1);
-    if (t_ < both) {
-      par = t_ & 1;
-      cc = t_ >> 1;
+  TS_DEV Tile tile(int tile) const {
+    Tile ti;
+    int m, lt, fb;
+    decode(tile, m, lt, fb);
+    nch(m, ti.n0, ti.n1);
+    const int i = m * nLT + lt;
+    ti.cs = tc->syn_cs ? tc->syn_cs[i] : 0;
+    ti.T = (tc->syn_zero && tc->syn_zero[i]) ? 0 : ti.n0 + ti.n1 - 2 * ti.cs;
+    ti.q = qimg + ((long)tc->chunk_prefix[m] * nfb + fb) * 16384;
+    ti.b = tc->synth + tc->synth_off[m] + (long)lt * 2 * NL * 128;
+    return ti;
+  }
+  // parity and chunk-of-parity of stage t_ (after the skipped pairs)
+  TS_DEV void parcc(const Tile &ti, int t_, int &par, int &cc) const {
+    const int t = t_ + 2 * ti.cs;
+    const int mn = min(ti.n0, ti.n1), both = 2 * mn;
+    if (t < both) {
+      par = t & 1;
+      cc = t >> 1;
     } else {
-      par = n0 > n1 ? 0 : 1;
-      cc = (t_ - both) + min(n0, n1);
+      par = ti.n0 > ti.n1 ? 0 : 1;
+      cc = (t - both) + mn;
     }
   }
-  // leading (parity 0, parity 1) degree-chunk pairs of tile (m, lt) whose
-  // table values are all negligible (the polar skip); the stage index t_ of
-  // the remaining stages maps to t_ + 2 cs in the full sequence
-  TS_DEV int cs(int m, int lt) const { return tc->syn_cs ? tc->syn_cs[m * nLT + lt] : 0; }
-  TS_DEV int stages(int tile) const {
-    int m, lt, fb, n0, n1;
-    decode(tile, m, lt, fb);
-    if (tc->syn_zero && tc->syn_zero[m * nLT + lt]) return 0;  // polar tile: zeros
-    nch(m, n0, n1);
-    return n0 + n1 - 2 * cs(m, lt);
+  TS_DEV int stages(const Tile &ti) const { return ti.T; }
+  TS_DEV int stages(int t) const { return tile(t).T; }
+  TS_DEV unsigned table_bytes(const Tile &) const { return 2u * NL * 128; }
+  TS_DEV int n(const Tile &) const { return NL; }
+  TS_DEV const char *a_src(const Tile &ti, int t_) const {
+    int par, cc;
+    parcc(ti, t_, par, cc);
+    return ti.q + (long)((par ? ti.n0 : 0) + cc) * nfb * 16384;
   }
-  TS_DEV unsigned table_bytes(int) const { return 2u * NL * 128; }
-  TS_DEV int n(int) const { return NL; }
-  TS_DEV const char *a_src(int tile, int t_) const {
-    int m, lt, fb, par, cc, n0, n1;
-    decode(tile, m, lt, fb);
-    parcc(m, t_ + 2 * cs(m, lt), par, cc);
-    nch(m, n0, n1);
-    return qimg + ((long)(tc->chunk_prefix[m] + (par ? n0 : 0) + cc) * nfb + fb) * 16384;
+  TS_DEV const char *b_src(const Tile &ti, int t_) const {
+    int par, cc;
+    parcc(ti, t_, par, cc);
+    return ti.b + (long)((par ? ti.n0 : 0) + cc) * nLT * 2 * NL * 128;
   }
-  TS_DEV const char *b_src(int tile, int t_) const {
-    int m, lt, fb, par, cc, n0, n1;
-    decode(tile, m, lt, fb);
-    parcc(m, t_ + 2 * cs(m, lt), par, cc);
-    nch(m, n0, n1);
-    const long bb = 2L * NL * 128;
-    return tc->synth + tc->synth_off[m] + (long)((par ? n0 : 0) + cc) * nLT * bb + (long)lt * bb;
-  }
-  TS_DEV int d_col(int tile, int t_) const {
-    int m, lt, fb, par, cc;
-    decode(tile, m, lt, fb);
-    parcc(m, t_ + 2 * cs(m, lt), par, cc);
+  TS_DEV int d_col(const Tile &ti, int t_) const {
+    int par, cc;
+    parcc(ti, t_, par, cc);
     return par * NL;
   }
-  TS_DEV bool first(int tile, int t_) const {
-    int m, lt, fb, par, cc;
-    decode(tile, m, lt, fb);
-    const int c = cs(m, lt);
-    parcc(m, t_ + 2 * c, par, cc);
-    return cc == c;
+  TS_DEV bool first(const Tile &ti, int t_) const {
+    int par, cc;
+    parcc(ti, t_, par, cc);
+    return cc == ti.cs;
   }
 };
 
@@ -645,6 +650,14 @@ struct TsAnalysSched {
   const TsTcTab *tc;
   int lmax, mmax, nfb, ntile;
   const char *wimg;
+  struct Tile {
+    int cnt;        // degrees of the tile
+    int T;          // stages that run (latitude chunks after the polar skip)
+    unsigned tb;    // table bytes per stage
+    int n;          // MMA N
+    const char *w;  // W image block of the first chunk that runs
+    const char *b;  // table block of the first chunk that runs
+  };
   TS_DEV int ntiles() const { return (mmax + 1) * 2 * ntile * nfb; }
   TS_DEV void decode(int tile, int &m, int &par, int &lt, int &fb) const {
     m = tile / (2 * ntile * nfb);
@@ -659,29 +672,29 @@ struct TsAnalysSched {
     decode(tile, m, par, lt, fb);
     return ts_atile_count(lmax, m, par, lt, tc->LTL);
   }
-  // leading latitude chunks skipped (their table values are all negligible)
-  TS_DEV int c0(int tile) const {
-    if (!tc->ana_c0) return 0;
+  TS_DEV Tile tile(int tile) const {
+    Tile ti;
     int m, par, lt, fb;
     decode(tile, m, par, lt, fb);
-    return tc->ana_c0[(2 * m + par) * tc->ntile + lt];
+    ti.cnt = ts_atile_count(lmax, m, par, lt, tc->LTL);
+    // leading latitude chunks skipped (their table values are all negligible)
+    const int c0 = tc->ana_c0 ? tc->ana_c0[(2 * m + par) * tc->ntile + lt] : 0;
+    ti.T = ti.cnt > 0 ? tc->nLC - c0 : 0;
+    ti.n = max(16, ts_round16(ti.cnt));
+    ti.tb = 2u * ti.n * 128;
+    ti.w = wimg + ((((long)m * nfb + fb) * 2 + par) * tc->nLC + c0) * 16384;
+    ti.b = ti.T > 0 ? tc->anal + ts_atile_offset(*tc, lmax, m, par, lt) + (long)c0 * ti.tb
+                    : tc->anal;
+    return ti;
   }
-  TS_DEV int stages(int tile) const { return cnt(tile) > 0 ? tc->nLC - c0(tile) : 0; }
-  TS_DEV int n(int tile) const { return max(16, ts_round16(cnt(tile))); }
-  TS_DEV unsigned table_bytes(int tile) const { return 2u * n(tile) * 128; }
-  TS_DEV const char *a_src(int tile, int c) const {
-    int m, par, lt, fb;
-    decode(tile, m, par, lt, fb);
-    return wimg + ((((long)m * nfb + fb) * 2 + par) * tc->nLC + c + c0(tile)) * 16384;
-  }
-  TS_DEV const char *b_src(int tile, int c) const {
-    int m, par, lt, fb;
-    decode(tile, m, par, lt, fb);
-    return tc->anal + ts_atile_offset(*tc, lmax, m, par, lt) +
-           (long)(c + c0(tile)) * table_bytes(tile);
-  }
-  TS_DEV int d_col(int, int) const { return 0; }
-  TS_DEV bool first(int, int c) const { return c == 0; }
+  TS_DEV int stages(const Tile &ti) const { return ti.T; }
+  TS_DEV int stages(int t) const { return tile(t).T; }
+  TS_DEV int n(const Tile &ti) const { return ti.n; }
+  TS_DEV unsigned table_bytes(const Tile &ti) const { return ti.tb; }
+  TS_DEV const char *a_src(const Tile &ti, int c) const { return ti.w + (long)c * 16384; }
+  TS_DEV const char *b_src(const Tile &ti, int c) const { return ti.b + (long)c * ti.tb; }
+  TS_DEV int d_col(const Tile &, int) const { return 0; }
+  TS_DEV bool first(const Tile &, int c) const { return c == 0; }
 };
 
 // grid = min(#SMs, tiles), block = 320, persistent.  Tiles with no l values
