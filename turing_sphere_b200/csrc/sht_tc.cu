@@ -151,6 +151,7 @@ struct ts_tc_tables {
   int *chunk_prefix = nullptr, *chunk_m = nullptr, *chunk_pc = nullptr;
   unsigned char *syn_zero = nullptr, *syn_cs = nullptr;
   int *ana_c0 = nullptr;
+  int *w_c0 = nullptr;  // per (m, parity): the smallest ana_c0 of its tiles
   // synthesis tiles, synthesis degree chunks and analysis latitude chunks the polar skip drops
   int skip_syn = 0, skip_syn_chunks = 0, skip_ana = 0;
   ts_dbuf qimg, wimg, gscratch;  // operand images and a G scratch of the standalone transforms
@@ -277,6 +278,15 @@ void tc_polar_skip(ts_plan p, ts_tc_tables *t, const std::vector<long> &soff,
       seen[tl] = 1;
   }
   for (int tl = 0; tl < ntiles; tl++) t->skip_ana += c0[tl];
+  std::vector<int> wc0(2 * M, nLC);
+  for (int tl = 0; tl < ntiles; tl++) {
+    const int mp = tl / t->ntile;  // 2 m + parity
+    // tiles without degrees (cnt 0) read nothing; the others bound it
+    const int m = mp / 2, par = mp % 2, lt = tl % t->ntile;
+    if (lt * LTL < kpar_h(p->lmax, m, par)) wc0[mp] = std::min(wc0[mp], c0[tl]);
+  }
+  TS_CUDA(cudaMalloc(&t->w_c0, sizeof(int) * wc0.size()));
+  TS_CUDA(cudaMemcpy(t->w_c0, wc0.data(), sizeof(int) * wc0.size(), cudaMemcpyHostToDevice));
   for (int i = 0; i < M * nLT; i++)
     if (!zero[i]) t->skip_syn_chunks += 2 * csk[i];
   TS_CUDA(cudaMalloc(&t->syn_cs, csk.size()));
@@ -372,7 +382,7 @@ void ts_tc_free(ts_plan p) {
   if (!t) return;
   for (void *q : {(void *)t->synth, (void *)t->anal, (void *)t->synth_off, (void *)t->anal_off,
                   (void *)t->err, (void *)t->chunk_prefix, (void *)t->chunk_m, (void *)t->chunk_pc,
-                  (void *)t->syn_zero, (void *)t->syn_cs, (void *)t->ana_c0})
+                  (void *)t->syn_zero, (void *)t->syn_cs, (void *)t->ana_c0, (void *)t->w_c0})
     if (q) cudaFree(q);
   t->qimg.release();
   t->wimg.release();
@@ -388,6 +398,11 @@ void ts_tc_set_fault(ts_plan p, int stall_copies, unsigned wait_limit) {
   t.stall_copies = stall_copies;
   t.wait_limit = wait_limit;
 }
+const int *ts_tc_w_c0(ts_plan p) {
+  const auto *t = static_cast<ts_tc_tables *>(p->tc);
+  return t ? t->w_c0 : nullptr;
+}
+
 void ts_tc_skip_counts(ts_plan p, int *tiles, int *chunks) {
   const auto *t = static_cast<ts_tc_tables *>(p->tc);
   *tiles = t ? t->skip_syn : 0;
