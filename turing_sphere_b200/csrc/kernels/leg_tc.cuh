@@ -16,10 +16,10 @@
 // precomputed image and the data operand from a raw-fp32 image of the same
 // byte layout (TsTcImg; written by a relayout kernel for the synthesis and by
 // the Fourier analysis itself for the analysis).  The kernels are persistent
-// (one CTA per SM walking tiles blockIdx.x + k*gridDim.x) with 320 threads in
+// (one CTA per SM walking tiles blockIdx.x + k*gridDim.x) with 448 threads in
 // fixed roles: warps 0-3 split each data tile in place into rna-rounded TF32
 // hi and lo, warp 4 issues the copies (expect-tx mbarriers over an S-slot
-// ring), warp 5 issues the MMAs, warps 6-9 drain the accumulators.  Tensor
+// ring), warp 5 issues the MMAs, warps 6-13 drain the accumulators.  Tensor
 // memory holds two accumulator buffers, so the epilogue of tile i overlaps the
 // MMAs of tile i+1 and the operand ring streams across tile boundaries.
 // Every wait is bounded: on timeout the kernel records an error flag, waits
@@ -358,10 +358,11 @@ TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes
 }
 
 // Persistent schedule.  The CTA takes tiles blockIdx.x, blockIdx.x +
-// gridDim.x, ...; `Sched` maps a tile to its stage count and, per stage, the
-// data tile, the table chunk and the accumulator column; every role walks the
+// gridDim.x, ...; `Sched` maps a tile to a descriptor (sc.tile: stage count,
+// bases, skip offsets, computed once per tile) and, per stage, the data
+// tile, the table chunk and the accumulator column; every role walks the
 // same sequence, so ring slots and barrier phases stay in step.  Warps 0-3
-// split data tiles, warp 4 copies, warp 5 issues MMAs, warps 6-9 drain the
+// split data tiles, warp 4 copies, warp 5 issues MMAs, warps 6-13 drain the
 // accumulators through `epilogue(tile, tmem_cols_of_buffer)`.
 template <class Sched, class Epilogue>
 TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes, unsigned tmem,
@@ -444,7 +445,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
   }
 }
 
-// rows 32*(warp%4) .. of TMEM belong to epilogue warp `warp` (warps 6-9)
+// rows 32*(warp%4) .. of TMEM belong to epilogue warp `warp` (warps 6-13)
 TS_DEV int ts_epi_row(int warp, int lane) { return (warp & 3) * 32 + lane; }
 
 // ----------------------------------------------------------------- synthesis
@@ -697,8 +698,9 @@ struct TsAnalysSched {
   TS_DEV bool first(const Tile &, int c) const { return c == 0; }
 };
 
-// grid = min(#SMs, tiles), block = 320, persistent.  Tiles with no l values
-// have no stages; their epilogue does nothing.  Dynamic shared memory:
+// grid = min(#SMs, tiles), block = 448, persistent.  Tiles with no l values
+// have no stages; their epilogue does nothing; tiles whose latitude chunks
+// the polar skip drops entirely write zeros.  Dynamic shared memory:
 // S*(2*16384 + 2*Nmax*128) + 2*min(Nmax, TS_TC_ANA_COLS)*2*TS_TC_ANA_ROW*4 + 1024
 // + sizeof(TsTcPipe).  TMEM:
 // two buffers of 256 columns.
