@@ -180,3 +180,18 @@ def test_polar_skip_drops_work_not_accuracy(device, lmax, nlat, nphi):
     qa = plan.analys(s32)
     assert O.rel_l2(qa[start:], q64[start:]) < TOL
     plan.status()
+
+
+def test_tc_lmax1023_parity(device):
+    """The largest grid of the SHT configuration (lmax 1023 on 1536 x 3072):
+    one field each way against the f64 oracle, with the polar skip active."""
+    lmax, nlat, nphi = 1023, 1536, 3072
+    plan = tc_plan(device, lmax, nlat, nphi)
+    assert plan.shapes["tc_skip_chunks"] > 0
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = scaled_spectrum(lmax, lmax, 5)
+    s64 = ref.synth(q.astype(np.float64))
+    assert O.rel_l2(plan.synth(q), s64) < TOL
+    s32 = s64.astype(np.float32)
+    assert O.rel_l2(plan.analys(s32), ref.analys(s32.astype(np.float64))) < TOL
+    plan.status()
