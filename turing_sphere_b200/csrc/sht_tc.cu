@@ -448,32 +448,54 @@ int ts_tc_ctas(ts_plan p, long ntiles) {
 namespace {
 
 // Q (fields) -> raw fp32 synthesis image; grid = (nchunks, q_nfb), block =
-// 256: warp -> 8 fields, lane -> k (coalesced 128-byte image rows).  A thread
-// issues the loads of all its 8 fields before its first store, so 8 loads
-// per thread are in flight instead of one.
+// 256: warp -> 8 fields, lane -> k (coalesced 128-byte image rows).  The CTA
+// of a parity-0 chunk also writes the parity-1 chunk of the same k range
+// (degrees m + 2j and m + 2j + 1 are adjacent, one 16-byte load when
+// aligned); parity-1 CTAs leave at once.  A thread issues the loads of all
+// its 8 fields before its first store, so 8 loads per thread are in flight.
 __global__ void ts_k_qimage(TsLegTab t, TsTcTab tc, TsFields q, int nfields, char *img,
                             int nfb) {
   constexpr int NF = TS_TC_FIELDS / 8;  // fields per thread
   const int c = blockIdx.x, fb = blockIdx.y;
-  const int m = tc.chunk_m[c], pc = tc.chunk_pc[c];
-  const int par = pc >> 16, cc = pc & 0xffff;
-  const int kp = ts_kpar(t.lmax, m, par);
+  const int pc = tc.chunk_pc[c];
+  if (pc >> 16) return;  // parity-1 chunks are written with their parity-0 partner
+  const int m = tc.chunk_m[c], cc = pc & 0xffff;
+  const int kp0 = ts_kpar(t.lmax, m, 0), kp1 = ts_kpar(t.lmax, m, 1);
+  const int n0 = (kp0 + TS_TC_KCH - 1) / TS_TC_KCH, n1 = (kp1 + TS_TC_KCH - 1) / TS_TC_KCH;
   const long base = ts_lm_base(t.lmax, m);
-  char *blk = img + ((long)c * nfb + fb) * 16384;
+  char *blk0 = img + ((long)c * nfb + fb) * 16384;
+  const bool has1 = cc < n1;
+  char *blk1 = img + ((long)(tc.chunk_prefix[m] + n0 + cc) * nfb + fb) * 16384;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int j = cc * TS_TC_KCH + lane;
-  float2 v[NF];
+  const bool v0 = j < kp0, v1 = j < kp1;
+  float2 a[NF], b[NF];
 #pragma unroll
   for (int i = 0; i < NF; i++) {
     const int f = fb * TS_TC_FIELDS + warp + 8 * i;
-    v[i] = make_float2(0.f, 0.f);
-    if (f < nfields && j < kp) v[i] = __ldg(ts_field(q, f) + base + par + 2 * j);
+    a[i] = b[i] = make_float2(0.f, 0.f);
+    if (f < nfields && v0) {
+      // degrees l = m + 2j (parity 0) and m + 2j + 1 (parity 1) are adjacent
+      const float2 *src = ts_field(q, f) + base + 2 * j;
+      if (v1 && (reinterpret_cast<unsigned long long>(src) & 15) == 0) {
+        const float4 x = __ldg(reinterpret_cast<const float4 *>(src));
+        a[i] = make_float2(x.x, x.y);
+        b[i] = make_float2(x.z, x.w);
+      } else {
+        a[i] = __ldg(src);
+        if (v1) b[i] = __ldg(src + 1);
+      }
+    }
   }
 #pragma unroll
   for (int i = 0; i < NF; i++) {
     const int fl = warp + 8 * i;
-    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl, lane)) = v[i].x;
-    *reinterpret_cast<float *>(blk + ts_swz_img(2 * fl + 1, lane)) = v[i].y;
+    *reinterpret_cast<float *>(blk0 + ts_swz_img(2 * fl, lane)) = a[i].x;
+    *reinterpret_cast<float *>(blk0 + ts_swz_img(2 * fl + 1, lane)) = a[i].y;
+    if (has1) {
+      *reinterpret_cast<float *>(blk1 + ts_swz_img(2 * fl, lane)) = b[i].x;
+      *reinterpret_cast<float *>(blk1 + ts_swz_img(2 * fl + 1, lane)) = b[i].y;
+    }
   }
 }
 
