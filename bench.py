@@ -150,6 +150,31 @@ def profiled_traffic(stage):
     return total if found else None
 
 
+def stage_roofline(stage, ms, alg_bytes, leg_flop, passes, hbm, bf16, of):
+    """Roofline of one pair stage (ms per launch): the larger of its HBM floor
+    (algorithmic bytes / bandwidth in GB/s) and, for a Legendre stage, its
+    tensor floor (`passes` split-TF32 passes of `leg_flop` at the dense TF32
+    rate bf16 / 2 TFLOP/s); `of` names the peaks' source."""
+    dur = ms / 1e3
+    t_hbm = alg_bytes / (hbm * 1e9)
+    t_tc = passes * leg_flop / (bf16 / 2 * 1e12) if stage.startswith("leg") else 0.0
+    if t_tc > t_hbm:
+        return {"kernel": stage, "bound": "tensor", "achieved": leg_flop / dur / 1e12,
+                "peak": bf16 / 2, "unit": "TFLOP/s", "frac": leg_flop / dur / 1e12 / (bf16 / 2),
+                "peak_source": f"bf16_tflops / 2, the dense TF32 rate ({of})",
+                "algorithmic_flop": leg_flop}
+    r = {"kernel": stage, "bound": "hbm", "achieved": alg_bytes / dur / 1e9, "peak": hbm,
+         "unit": "GB/s", "frac": alg_bytes / dur / 1e9 / hbm, "peak_source": f"hbm_gbs ({of})",
+         "algorithmic_bytes": alg_bytes}
+    if stage.startswith("leg"):
+        r["tensor_floor_us"] = t_tc * 1e6
+        r["hbm_floor_us"] = t_hbm * 1e6
+        r["tensor_pipe_tflops"] = passes * leg_flop / dur / 1e12
+        r["note"] = (f"HBM-bound: moving its inputs and outputs takes longer than its "
+                     f"{passes} split-TF32 tensor passes at the dense TF32 rate")
+    return r
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -677,37 +702,16 @@ def main():
         passes = 3 if args.precision != "fp32" else 1
         of = "of measured" if src == "measured" else "of fallback"
 
-        def stage_roof(st):
-            """Roofline of one stage: the larger of its HBM floor (algorithmic
-            bytes / bandwidth) and, for a Legendre stage, its tensor floor
-            (the split-TF32 passes of its flops / the dense TF32 rate)."""
-            dur = stage_ms[st] / 1e3
-            t_hbm = alg_bytes[st] / (hbm * 1e9)
-            t_tc = passes * leg_flop / (bf16 / 2 * 1e12) if st.startswith("leg") else 0.0
-            if t_tc > t_hbm:
-                return {"kernel": st, "bound": "tensor", "achieved": leg_flop / dur / 1e12,
-                        "peak": bf16 / 2, "unit": "TFLOP/s",
-                        "frac": leg_flop / dur / 1e12 / (bf16 / 2),
-                        "peak_source": f"bf16_tflops / 2, the dense TF32 rate ({of})",
-                        "algorithmic_flop": leg_flop}
-            r = {"kernel": st, "bound": "hbm", "achieved": alg_bytes[st] / dur / 1e9,
-                 "peak": hbm, "unit": "GB/s", "frac": alg_bytes[st] / dur / 1e9 / hbm,
-                 "peak_source": f"hbm_gbs ({of})", "algorithmic_bytes": alg_bytes[st]}
-            if st.startswith("leg"):
-                r["tensor_floor_us"] = t_tc * 1e6
-                r["hbm_floor_us"] = t_hbm * 1e6
-                r["tensor_pipe_tflops"] = passes * leg_flop / dur / 1e12
-                r["note"] = (f"HBM-bound: moving its inputs and outputs takes longer than its "
-                             f"{passes} split-TF32 tensor passes at the dense TF32 rate")
-            return r
-
-        roof = stage_roof(name)
+        roof = stage_roofline(name, stage_ms[name], alg_bytes[name], leg_flop, passes, hbm, bf16,
+                              of)
         roof["traffic"] = profiled_traffic(name)
         roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                   "launch (profiles/sht_pair_lmax255_b256_kernels.txt)")
         roof["stage_ms"] = stage_ms
-        roof["stages"] = {st: {k: v for k, v in stage_roof(st).items()
-                               if k in ("bound", "achieved", "unit", "frac")} for st in stages}
+        roof["stages"] = {
+            st: {k: v for k, v in stage_roofline(st, stage_ms[st], alg_bytes[st], leg_flop, passes,
+                                                 hbm, bf16, of).items()
+                 if k in ("bound", "achieved", "unit", "frac")} for st in stages}
         cpu = cpu_baseline(lmax, nlat, nphi, budget_s=10.0, threads=0)
         one = cpu_baseline(lmax, nlat, nphi, budget_s=5.0, threads=1)
         cpu["single_thread"] = {k: one[k] for k in ("value", "cores", "sample")}
