@@ -5,7 +5,7 @@ transform batch) never exchange data during a step, so N GPUs each advance a
 contiguous block of the instances with no collective on the data path.  The
 only communication is at the edges: the maximum device time over ranks for
 reporting, and an optional gather of final states, losses or gradients to
-rank 0 (SURVEY (e): "one optional all-gather at the end").
+rank 0 once a run has finished.
 
 The helpers take any initialised torch.distributed process group: NCCL with
 CUDA tensors on a GPU node, gloo with CPU tensors in tests.
