@@ -49,8 +49,8 @@ def parse():
     ap.add_argument("--only", choices=["all", "sht", "imex"], default="all",
                     help="sht: the timed transform pairs alone; imex: the model steps alone "
                          "(short runs for a profiler's launch list)")
-    ap.add_argument("--skip-config1", action="store_true",
-                    help="with --only imex: leave out the 2000-step single-instance runs")
+    ap.add_argument("--skip-single", action="store_true",
+                    help="with --only imex: leave out the 2000-step single-instance lmax-63 runs")
     ap.add_argument("--no-autotune", action="store_true",
                     help="plans keep their default kernel shapes (no tuning launches, so a "
                          "profiler's launch skip count lands on the timed kernels)")
@@ -446,7 +446,7 @@ def time_e2e(plan, q0, qa, qb, spat, B, K, stream, world, dist):
     return ems, Ke, err
 
 
-def time_imex_config1(dev, stream, precision, K=2000, graphs=True):
+def time_imex_single_lmax63(dev, stream, precision, K=2000, graphs=True):
     """A single Schnakenberg instance at lmax 63 on the 96 x 192 Gauss grid,
     K steps: the launch-latency-bound case, run as captured step graphs
     (default) or eager launches.  Returns steps/s."""
@@ -474,7 +474,7 @@ def time_imex_config1(dev, stream, precision, K=2000, graphs=True):
     return K / (ms / 1e3)
 
 
-def time_config3(dev, stream, K=200):
+def time_brusselator_sweep(dev, stream, K=200):
     """Brusselator parameter sweep: 256 instances with (A, B) spread over the
     Turing-unstable band, lmax 127 on 192 x 384, tensor-core plan, steps as
     captured graphs.  Returns instance-steps/s."""
@@ -514,7 +514,7 @@ def time_config3(dev, stream, K=200):
 
 
 def time_ragged(dev, stream, K=100):
-    """Config 3's ragged variant: 64 Brusselator instances at each of lmax
+    """The ragged sweep: 64 Brusselator instances at each of lmax
     63/127/255 (96x192, 192x384, 384x768 grids, one plan and model each),
     advanced as one model group (one captured graph per step, the three
     models on concurrent branches).  Returns instance-steps/s over all 192."""
@@ -614,14 +614,15 @@ def main():
     if args.only == "imex":
         ni = args.imex_instances
         ims, launches, ok = time_imex(dev, plan, ni, args.imex_steps, max(3, args.warmup), stream)
-        c1 = {} if args.skip_config1 else {
-            g: time_imex_config1(dev, stream, "fp32", graphs=g) for g in (True, False)}
+        c1 = {} if args.skip_single else {
+            g: time_imex_single_lmax63(dev, stream, "fp32", graphs=g) for g in (True, False)}
         if rank == 0:
             print(json.dumps({"only": "imex", "instances": ni, "launches_per_step": launches,
                               "ms_per_step": ims / args.imex_steps, "finite": ok,
                               "value": world * ni * args.imex_steps / (ims / 1e3),
                               "unit": "instance-steps/s",
-                              "config1_steps_per_s": {"graphs": c1.get(True), "eager": c1.get(False)}}),
+                              "single_lmax63_steps_per_s": {"graphs": c1.get(True),
+                                                              "eager": c1.get(False)}}),
                   flush=True)
         return finish(plan, plain, dev, world)
 
@@ -679,9 +680,9 @@ def main():
     ni = args.imex_instances
     imex_tc_ms, imex_launches, ok_tc = time_imex(dev, plan, ni, args.imex_steps, 3, stream)
     imex_fp_ms, _, ok_fp = time_imex(dev, plain, ni, max(10, args.imex_steps // 4), 3, stream)
-    c1_fp32 = time_imex_config1(dev, stream, "fp32")
-    c1_tc = time_imex_config1(dev, stream, "tf32x3")
-    c3 = time_config3(dev, stream)
+    c1_fp32 = time_imex_single_lmax63(dev, stream, "fp32")
+    c1_tc = time_imex_single_lmax63(dev, stream, "tf32x3")
+    c3 = time_brusselator_sweep(dev, stream)
     c3["ragged"] = time_ragged(dev, stream)
     a4_s, a4_ok = time_adjoint(dev, "allencahn", 255, 384, 768, 1, 256, 32)
     a5_s, a5_ok = time_adjoint(dev, "schnakenberg", 511, 768, 1536, 64, 64, 32)
@@ -740,15 +741,15 @@ def main():
                      "tc_steps_per_s_per_instance": args.imex_steps / (imex_tc_ms / 1e3),
                      "fp32_steps_per_s": world * ni * max(10, args.imex_steps // 4) / (imex_fp_ms / 1e3),
                      "unit": "instance-steps/s", "finite": ok_tc and ok_fp,
-                     "config1": {"workload": "1 Schnakenberg instance, lmax 63, 96x192, "
+                     "single_lmax63": {"workload": "1 Schnakenberg instance, lmax 63, 96x192, "
                                              "2000 steps as captured step graphs",
                                  "fp32_steps_per_s": c1_fp32, "tc_steps_per_s": c1_tc}},
-            "config3": c3,
+            "brusselator_sweep_lmax127": c3,
             "adjoint": {
-                "config4": {"workload": "Allen-Cahn, 1 instance, lmax 255, 384x768, tf32x3, "
+                "allencahn_lmax255": {"workload": "Allen-Cahn, 1 instance, lmax 255, 384x768, tf32x3, "
                                         "256 steps forward + adjoint, checkpoints every 32",
                             "steps_per_s": 256 / a4_s, "finite": a4_ok},
-                "config5": {"workload": "Schnakenberg, 64 instances, lmax 511, 768x1536, "
+                "schnakenberg_lmax511": {"workload": "Schnakenberg, 64 instances, lmax 511, 768x1536, "
                                         "tf32x3, 64 steps forward + adjoint, checkpoints every 32, "
                                         "gradients w.r.t. (a, b, D1, D2, dt) and the state",
                             "instance_steps_per_s": 64 * 64 / a5_s, "finite": a5_ok},

@@ -42,7 +42,7 @@ def rel(a, b):
 
 @pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
 def test_allencahn_grid_loss_gradients(device, precision):
-    """Config 4 in small: Allen-Cahn, L = ||u(T) - u_target||^2 on the grid,
+    """The Allen-Cahn adjoint workload in small: Allen-Cahn, L = ||u(T) - u_target||^2 on the grid,
     gradients w.r.t. the initial coefficients (two random directions) and
     eps2, with checkpoints every 8 of 20 steps."""
     model = mModelByKey("allencahn")
@@ -85,7 +85,7 @@ def test_allencahn_grid_loss_gradients(device, precision):
 
 
 def test_schnakenberg_batched_parameter_gradients(device):
-    """Config 5 in small: two Schnakenberg instances with their own
+    """The Schnakenberg sweep adjoint in small: two Schnakenberg instances with their own
     parameters, L = sum_k <w_k, (U_T, V_T)_k>; per-instance gradients
     w.r.t. (a, b, D1, D2) and the initial state, checkpoints every 5 of 12."""
     model = mModelByKey("schnakenberg")

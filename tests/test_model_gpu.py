@@ -152,7 +152,7 @@ def test_oversample_measure_and_setoversample(device):
 
 
 def spectral_seed(lmax, p, seed, amp=1e-2):
-    """Config-1 seeding: the homogeneous state u* = a+b, v* = b/(a+b)^2 in the
+    """Spectral seeding of the single-instance run: the homogeneous state u* = a+b, v* = b/(a+b)^2 in the
     l = 0 coefficient (times sqrt(4 pi)) plus N(0, amp^2) on every
     coefficient with 1 <= l <= lmax (m = 0 imaginary parts zero)."""
     rng = np.random.default_rng(seed)
@@ -175,7 +175,7 @@ def spectral_seed(lmax, p, seed, amp=1e-2):
 
 @pytest.mark.parametrize("nsteps", [20, 1000])
 def test_schnakenberg_run_matches_f64_oracle(device, nsteps):
-    """Config 1 (lmax 63, 96 x 192 Gauss grid): the fp32 GPU run against the
+    """A single Schnakenberg instance (lmax 63, 96 x 192 Gauss grid): the fp32 GPU run against the
     f64 oracle driving the same IMEX step; <= 1e-4 relative L2 per field."""
     model = mModelByKey("schnakenberg")
     p = defaultParams(model)
