@@ -60,6 +60,10 @@ struct Stage {
   int threads = 0;    // phase: threads per CTA (two-phase FFT: P*R, lb = R rows)
   bool wimg = false;  // tensor-core plan: the phase writes the W image itself
   size_t smem = 0;
+  // SpecEW: the variant that takes four consecutive coefficients per thread
+  // (float4 loads and stores; used when every array and stride allows it)
+  std::string expr_v4;
+  cudaKernel_t kern_v4 = nullptr;
   std::string label;  // one line, for describe()
   std::string src;    // generated CUDA of this stage
 };
@@ -344,6 +348,46 @@ void schedule(ts_model m, Program &P, bool is_step) {
           src << "  io.sout[" << o << "][inst * io.sout_stride[" << o << "] + idx] = v" << outs[o]
               << ";\n";
         src << "}\n";
+        // the same statements on four consecutive coefficients per thread
+        {
+          Emitter ev{f, {}};
+          src << "extern \"C\" __global__ void __launch_bounds__(256) " << kn << "_v4"
+              << "(TsSpecIO io) {\n"
+              << "  const long i4 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 4;\n"
+              << "  if (i4 >= io.n) return;\n  const long inst = blockIdx.y;\n"
+              << "  const float *prm = io.prm + inst * io.nprm;\n"
+              << ev.scalars();
+          int kk = 0;
+          for (int v : ins) {
+            src << "  const float4 x" << kk << " = *reinterpret_cast<const float4 *>(io.sin[" << kk
+                << "] + inst * io.sin_stride[" << kk << "] + i4);\n";
+            src << "  const float a" << kk << "[4] = {x" << kk << ".x, x" << kk << ".y, x" << kk
+                << ".z, x" << kk << ".w};\n";
+            kk++;
+          }
+          for (size_t o = 0; o < outs.size(); o++) src << "  float r" << o << "[4];\n";
+          src << "#pragma unroll\n  for (int u = 0; u < 4; u++) {\n";
+          kk = 0;
+          for (int v : ins) {
+            ev.name[v] = "v" + std::to_string(v);
+            src << "    const float v" << v << " = a" << kk << "[u];\n";
+            kk++;
+          }
+          for (int i : grp) {
+            const auto &s2 = f.body[i];
+            src << "    const float v" << s2.out << " = " << ev.e(s2.expr) << ";\n";
+            ev.name[s2.out] = "v" + std::to_string(s2.out);
+          }
+          for (size_t o = 0; o < outs.size(); o++)
+            src << "    r" << o << "[u] = v" << outs[o] << ";\n";
+          src << "  }\n";
+          for (size_t o = 0; o < outs.size(); o++)
+            src << "  *reinterpret_cast<float4 *>(io.sout[" << o << "] + inst * io.sout_stride[" << o
+                << "] + i4) = make_float4(r" << o << "[0], r" << o << "[1], r" << o << "[2], r" << o
+                << "[3]);\n";
+          src << "}\n";
+          st.expr_v4 = kn + "_v4";
+        }
         st.expr = kn;
         st.label = "kernel  " + std::to_string(grp.size()) + " spectral statement(s)";
         st.src = src.str();
@@ -677,6 +721,7 @@ void compile_kernels(ts_model m) {
       if (s.expr.empty()) continue;
       const std::string name = lowered.count(s.expr) ? lowered[s.expr] : s.expr;
       TS_CUDA(cudaLibraryGetKernel(&s.kern, m->lib, name.c_str()));
+      if (!s.expr_v4.empty()) TS_CUDA(cudaLibraryGetKernel(&s.kern_v4, m->lib, s.expr_v4.c_str()));
       if (s.smem > 48 * 1024)
         TS_CUDA(cudaKernelSetAttributeForDevice(
             s.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem, m->ctx->device));
@@ -790,8 +835,20 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
         TsSpecIO io;
         fill_spec_io(m, P, s, io);
         void *args[] = {&io};
-        dim3 grid((unsigned)((2 * p->nlm + 255) / 256), B);
-        TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(256), args, 0, st));
+        // four coefficients per thread when every array start and stride is
+        // a multiple of four floats (16-byte loads and stores)
+        bool v4 = s.kern_v4 && io.n % 4 == 0;
+        for (size_t i = 0; i < s.in.size() && v4; i++)
+          v4 = io.sin_stride[i] % 4 == 0 && (reinterpret_cast<uintptr_t>(io.sin[i]) & 15) == 0;
+        for (size_t i = 0; i < s.out.size() && v4; i++)
+          v4 = io.sout_stride[i] % 4 == 0 && (reinterpret_cast<uintptr_t>(io.sout[i]) & 15) == 0;
+        if (v4) {
+          dim3 grid((unsigned)((io.n / 4 + 255) / 256), B);
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern_v4, grid, dim3(256), args, 0, st));
+        } else {
+          dim3 grid((unsigned)((2 * p->nlm + 255) / 256), B);
+          TS_CUDA(cudaLaunchKernel((const void *)s.kern, grid, dim3(256), args, 0, st));
+        }
         break;
       }
     }
