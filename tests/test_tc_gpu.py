@@ -24,6 +24,8 @@ def tc_plan(device, lmax, nlat, nphi, mmax=None):
     (63, 96, 192, 63, 3),
     (127, 192, 384, 127, 70),     # two 64-field blocks, the second partial
     (255, 384, 768, 255, 2),      # one 192-latitude tile
+    (255, 384, 768, 255, 16),     # the SHT configuration's batch sizes 16 and 256
+    (255, 384, 768, 255, 256),
     (31, 33, 64, 31, 2),          # odd nlat: the equator row
     (40, 48, 96, 20, 5),          # mmax < lmax
 ])
