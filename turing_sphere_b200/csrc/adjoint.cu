@@ -19,17 +19,31 @@
 namespace {
 
 // grid[f][lat][phi] *= w(lat) (mul) or /= w(lat); w is stored for the
-// northern half and mirrored
+// northern half and mirrored.  grid = (nlat, fields): one row per CTA, its
+// weight read once, 16-byte accesses when the row allows them.
 __global__ void ts_k_scale_grid(float *out, const float *in, const float *__restrict__ wq,
-                                int nlat, int nphi, int nh, long nf, int mul) {
-  const long npts = (long)nlat * nphi;
-  const long total = npts * nf;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long)gridDim.x * blockDim.x) {
-    const int lat = (int)((i % npts) / nphi);
-    const int h = lat < nh ? lat : nlat - 1 - lat;
-    const float w = wq[h];
-    out[i] = mul ? in[i] * w : in[i] / w;
+                                int nlat, int nphi, int nh, int mul) {
+  const int lat = blockIdx.x;
+  const int h = lat < nh ? lat : nlat - 1 - lat;
+  const float w = wq[h];
+  const long off = ((long)blockIdx.y * nlat + lat) * nphi;
+  const float *src = in + off;
+  float *dst = out + off;
+  if ((nphi & 3) == 0 && ((reinterpret_cast<unsigned long long>(src) |
+                           reinterpret_cast<unsigned long long>(dst)) & 15) == 0) {
+    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+    float4 *d4 = reinterpret_cast<float4 *>(dst);
+    for (int i = threadIdx.x; i < (nphi >> 2); i += blockDim.x) {
+      float4 v = s4[i];
+      if (mul) {
+        v.x *= w; v.y *= w; v.z *= w; v.w *= w;
+      } else {
+        v.x /= w; v.y /= w; v.z /= w; v.w /= w;
+      }
+      d4[i] = v;
+    }
+  } else {
+    for (int i = threadIdx.x; i < nphi; i += blockDim.x) dst[i] = mul ? src[i] * w : src[i] / w;
   }
 }
 
@@ -50,10 +64,8 @@ __global__ void ts_k_scale_spec(float2 *out, const float2 *in, int lmax, int mma
 }
 
 void scale_grid(ts_plan p, float *out, const float *in, int nf, bool mul, cudaStream_t s) {
-  const long total = (long)p->nlat * p->nphi * nf;
-  const int blocks = (int)std::min<long>((total + 255) / 256, 148L * 16);
-  ts_k_scale_grid<<<blocks, 256, 0, s>>>(out, in, p->d_wq, p->nlat, p->nphi, p->nh, nf,
-                                         mul ? 1 : 0);
+  dim3 grid(p->nlat, nf);
+  ts_k_scale_grid<<<grid, 256, 0, s>>>(out, in, p->d_wq, p->nlat, p->nphi, p->nh, mul ? 1 : 0);
   TS_CUDA(cudaGetLastError());
 }
 

@@ -1144,9 +1144,23 @@ TsAdjIO adj_io(ts_model m, const AdjStmt &as) {
 }
 
 __global__ void ts_k_axpy(float *y, const float *x, long n) {
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x)
-    y[i] += x[i];
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x, step = (long)gridDim.x * blockDim.x;
+  if ((n & 3) == 0 && ((reinterpret_cast<unsigned long long>(y) |
+                        reinterpret_cast<unsigned long long>(x)) & 15) == 0) {
+    float4 *y4 = reinterpret_cast<float4 *>(y);
+    const float4 *x4 = reinterpret_cast<const float4 *>(x);
+    for (long i = t; i < (n >> 2); i += step) {
+      float4 a = y4[i];
+      const float4 b = x4[i];
+      a.x += b.x;
+      a.y += b.y;
+      a.z += b.z;
+      a.w += b.w;
+      y4[i] = a;
+    }
+  } else {
+    for (long i = t; i < n; i += step) y[i] += x[i];
+  }
 }
 
 void axpy(float *y, const float *x, long n, cudaStream_t st) {
