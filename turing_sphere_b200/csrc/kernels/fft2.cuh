@@ -454,10 +454,13 @@ TS_DEV void ts_f2_store_rows(const float2 *b, float *__restrict__ dst, int nphi,
 // (a row without a latitude, or the equator's repeat, reads as zero), and
 // writes the folded, weighted values: with R/2 = 8 and lat0 a multiple of 8,
 // every (m, parity, re|im) run covers one whole 32-byte sector of the image.
-template <class C, bool SKIP>
+// w_kmin (null: none) holds, per 32-latitude chunk and parity, the order m
+// from which the polar-skipped analysis never reads that chunk: writes of
+// those (m, parity) blocks are left out.
+template <class C>
 TS_DEV void ts_f2_write_w(const float2 *b, int lat0, long f, const TsFftTab &ft,
                           const float *__restrict__ wq, char *wimg, int nfb, int fpb, int nlc,
-                          int nh, const int *__restrict__ w_c0) {
+                          int nh, const int *__restrict__ w_kmin) {
   constexpr int NPR = C::R / 2;
   const long fb = f / fpb;
   const int fl = (int)(f - fb * fpb);
@@ -478,15 +481,11 @@ TS_DEV void ts_f2_write_w(const float2 *b, int lat0, long f, const TsFftTab &ft,
   // disjoint banks (a bijection when 2P is a multiple of 16)
   const int g = threadIdx.x / NPR;
   const int k0 = (2 * C::P) % 16 == 0 ? (g & ~15) + ((g & 1) << 3) + ((g >> 1) & 7) : g;
-  for (int k = k0; k <= ft.mmax; k += 2 * C::P) {
-    // the polar skip never reads chunks below w_c0[2 k + parity] (SKIP: the
-    // standalone analysis; the model phase, short of registers, writes all)
-    bool e0 = true, e1 = true;
-    if constexpr (SKIP) {
-      e0 = !w_c0 || (lat >> 5) >= __ldg(w_c0 + 2 * k);
-      e1 = !w_c0 || (lat >> 5) >= __ldg(w_c0 + 2 * k + 1);
-      if (!e0 && !e1) continue;
-    }
+  const int kl0 = w_kmin ? __ldg(w_kmin + 2 * (lat >> 5)) : ft.mmax + 1;
+  const int kl1 = w_kmin ? __ldg(w_kmin + 2 * (lat >> 5) + 1) : ft.mmax + 1;
+  const int kend = min(ft.mmax + 1, max(kl0, kl1));
+  for (int k = k0; k < kend; k += 2 * C::P) {
+    const bool e0 = k < kl0, e1 = k < kl1;
     const float2 xn = ts_f2_xk<C>(rn, k, ft);
     const float2 xs = south ? ts_f2_xk<C>(rs, k, ft) : make_float2(0.f, 0.f);
     char *blk = base + k * kstep;
@@ -577,7 +576,7 @@ template <int P, int Q, int R>
 __global__ void __launch_bounds__(P *R, TS_F2_MINB(P, R))
 ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
                const float *__restrict__ wq, char *wimg, int nfb, int fpb, int nlc, int nh,
-               const int *__restrict__ w_c0) {
+               const int *__restrict__ w_kmin) {
   using C = TsF2<P, Q, R>;
   extern __shared__ float2 ts_smem_f2w[];
   float2 *twq = ts_smem_f2w;
@@ -588,7 +587,7 @@ ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
   ts_f2_twq<C>(twq, ft);
   __syncthreads();
   ts_f2_forward_in<C>(b, twq, spat + f * spat_stride, ft.nphi, rows);
-  ts_f2_write_w<C, true>(b, lat0, f, ft, wq, wimg, nfb, fpb, nlc, nh, w_c0);
+  ts_f2_write_w<C>(b, lat0, f, ft, wq, wimg, nfb, fpb, nlc, nh, w_kmin);
 }
 
 // ------------------------------------------------------- fused grid phase
@@ -726,8 +725,8 @@ ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
 #pragma unroll 1
   for (int k = 0; k < NANA; k++) {
     if constexpr (PAIRED)
-      ts_f2_write_w<C, false>(buf + k * BS, lat0, inst * NANA + k, ft, io.wq, io.wimg,
-                              io.w_nfb, io.w_fpb, io.w_nlc, io.nh, nullptr);
+      ts_f2_write_w<C>(buf + k * BS, lat0, inst * NANA + k, ft, io.wq, io.wimg, io.w_nfb,
+                       io.w_fpb, io.w_nlc, io.nh, io.w_kmin);
     else
       ts_f2_unpack<C>(buf + k * BS, io.gm + (inst * NANA + k) * io.field, ft, rows);
   }

@@ -158,6 +158,7 @@ struct TsPhaseIO {
   char *wimg;
   int w_nfb, w_fpb, w_nlc, nh;
   const float *wq;
+  const int *w_kmin;  // polar skip of W-image writes (see ts_f2_write_w; null: none)
 };
 
 // I/O of a model's generated adjoint kernels: the forward ("tape") kernel of

@@ -788,6 +788,7 @@ void run_program(ts_model m, Program &P, cudaStream_t st) {
           io.w_nfb = (B * s.nana + s.per_cta - 1) / s.per_cta;
           io.w_nlc = (p->nh + 31) / 32;
           io.wq = p->d_wq;
+          io.w_kmin = ts_tc_w_kmin(p);
         }
         TsFftTab ft = p->fft;
         void *args[] = {&ft, &io};

@@ -145,8 +145,9 @@ TsTcGeom ts_tc_geom(ts_plan p);
 void ts_tc_set_fault(ts_plan p, int stall_copies, unsigned wait_limit);
 // tiles / chunks the tensor-core polar skip drops
 void ts_tc_skip_counts(ts_plan p, int *tiles, int *chunks);
-// per (m, parity): W-image latitude chunks below it are never read (null: all are)
-const int *ts_tc_w_c0(ts_plan p);
+// per (32-latitude chunk, parity): the order m from which the W image's chunk
+// is never read (null: every chunk is read)
+const int *ts_tc_w_kmin(ts_plan p);
 int ts_tc_ctas(ts_plan p, long ntiles);
 // TC synthesis: fields -> q image (qbuf, or the plan's) -> fm
 void ts_launch_leg_synth_tc(ts_plan p, const TsFields &q, float2 *fm, long fm_stride, int nfields,

@@ -484,7 +484,7 @@ void f2_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb, char *w
   dim3 grid((p->nh + R / 2 - 1) / (R / 2), nf);
   ts_f2_analys_w<P, Q, R><<<grid, P * R, smem, s>>>(p->fft, spat, ss, p->d_wq, wimg,
                                                     (nf + fpb - 1) / fpb, fpb, nlc, p->nh,
-                                                    ts_tc_w_c0(p));
+                                                    ts_tc_w_kmin(p));
   TS_CUDA(cudaGetLastError());
 }
 }  // namespace

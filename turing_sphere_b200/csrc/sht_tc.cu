@@ -151,7 +151,7 @@ struct ts_tc_tables {
   int *chunk_prefix = nullptr, *chunk_m = nullptr, *chunk_pc = nullptr;
   unsigned char *syn_zero = nullptr, *syn_cs = nullptr;
   int *ana_c0 = nullptr;
-  int *w_c0 = nullptr;  // per (m, parity): the smallest ana_c0 of its tiles
+  int *w_kmin = nullptr;  // per (latitude chunk, parity): the m from which it is never read
   // synthesis tiles, synthesis degree chunks and analysis latitude chunks the polar skip drops
   int skip_syn = 0, skip_syn_chunks = 0, skip_ana = 0;
   ts_dbuf qimg, wimg, gscratch;  // operand images and a G scratch of the standalone transforms
@@ -285,8 +285,17 @@ void tc_polar_skip(ts_plan p, ts_tc_tables *t, const std::vector<long> &soff,
     const int m = mp / 2, par = mp % 2, lt = tl % t->ntile;
     if (lt * LTL < kpar_h(p->lmax, m, par)) wc0[mp] = std::min(wc0[mp], c0[tl]);
   }
-  TS_CUDA(cudaMalloc(&t->w_c0, sizeof(int) * wc0.size()));
-  TS_CUDA(cudaMemcpy(t->w_c0, wc0.data(), sizeof(int) * wc0.size(), cudaMemcpyHostToDevice));
+  // per (chunk, parity): the smallest m0 such that no tile of any m >= m0
+  // reads the chunk (the W writers leave those blocks out)
+  std::vector<int> kmin(2 * nLC, M);
+  for (int par = 0; par < 2; par++)
+    for (int ch = 0; ch < nLC; ch++) {
+      int m0 = M;
+      while (m0 > 0 && ch < wc0[2 * (m0 - 1) + par]) m0--;
+      kmin[2 * ch + par] = m0;
+    }
+  TS_CUDA(cudaMalloc(&t->w_kmin, sizeof(int) * kmin.size()));
+  TS_CUDA(cudaMemcpy(t->w_kmin, kmin.data(), sizeof(int) * kmin.size(), cudaMemcpyHostToDevice));
   for (int i = 0; i < M * nLT; i++)
     if (!zero[i]) t->skip_syn_chunks += 2 * csk[i];
   TS_CUDA(cudaMalloc(&t->syn_cs, csk.size()));
@@ -382,7 +391,7 @@ void ts_tc_free(ts_plan p) {
   if (!t) return;
   for (void *q : {(void *)t->synth, (void *)t->anal, (void *)t->synth_off, (void *)t->anal_off,
                   (void *)t->err, (void *)t->chunk_prefix, (void *)t->chunk_m, (void *)t->chunk_pc,
-                  (void *)t->syn_zero, (void *)t->syn_cs, (void *)t->ana_c0, (void *)t->w_c0})
+                  (void *)t->syn_zero, (void *)t->syn_cs, (void *)t->ana_c0, (void *)t->w_kmin})
     if (q) cudaFree(q);
   t->qimg.release();
   t->wimg.release();
@@ -398,9 +407,9 @@ void ts_tc_set_fault(ts_plan p, int stall_copies, unsigned wait_limit) {
   t.stall_copies = stall_copies;
   t.wait_limit = wait_limit;
 }
-const int *ts_tc_w_c0(ts_plan p) {
+const int *ts_tc_w_kmin(ts_plan p) {
   const auto *t = static_cast<ts_tc_tables *>(p->tc);
-  return t ? t->w_c0 : nullptr;
+  return t ? t->w_kmin : nullptr;
 }
 
 void ts_tc_skip_counts(ts_plan p, int *tiles, int *chunks) {
