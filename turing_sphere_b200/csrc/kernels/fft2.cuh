@@ -302,6 +302,67 @@ TS_DEV void ts_f2_inverse_out(float2 *b, const float2 *twq, float *__restrict__ 
   }
 }
 
+// grid rows leave shared memory by bulk copies (one per row, issued by one
+// thread; the async proxy reads the staging, so the writes are fenced first)
+TS_DEV void ts_f2_fence_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+TS_DEV void ts_f2_bulk_s2g(void *dst, const void *src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(
+                   reinterpret_cast<unsigned long long>(dst)),
+               "r"((unsigned)__cvta_generic_to_shared(src)), "r"(bytes)
+               : "memory");
+}
+TS_DEV void ts_f2_bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+TS_DEV void ts_f2_bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+// ts_f2_inverse whose second phase stages z in natural order (row pitch H,
+// 16-byte aligned rows) and writes each grid row with one bulk copy.  Needs
+// dst 16-byte aligned and nphi a multiple of 4 (the caller checks).
+template <class C, class LatOf>
+TS_DEV void ts_f2_inverse_bulk(float2 *b, const float2 *twq, float *__restrict__ dst, int nphi,
+                               LatOf lat_of) {
+  const int tid = threadIdx.x;
+  {
+    int r, k1;
+    ts_f2_rk<C>(tid, r, k1);
+    float2 *row = b + r * C::RP;
+    float2 x[C::Q];
+#pragma unroll
+    for (int k2 = 0; k2 < C::Q; k2++) x[k2] = row[k1 + C::P * k2];
+    ts_dft<C::Q, +1>(x);
+#pragma unroll
+    for (int n2 = 1; n2 < C::Q; n2++) x[n2] = c_mul(x[n2], twq[n2 * C::P1 + k1]);
+    __syncthreads();
+#pragma unroll
+    for (int n2 = 0; n2 < C::Q; n2++) row[n2 * C::P1 + k1] = x[n2];
+    __syncthreads();
+  }
+  const bool act = tid < C::Q * C::R;
+  const int r = tid / C::Q, n2 = tid - r * C::Q;
+  float2 x[C::P];
+  if (act) {
+    const float2 *row = b + r * C::RP;
+#pragma unroll
+    for (int k1 = 0; k1 < C::P; k1++) x[k1] = row[n2 * C::P1 + k1];
+    ts_dft<C::P, +1>(x);
+  }
+  __syncthreads();
+  if (act) {
+    float2 *srow = b + r * C::H;
+#pragma unroll
+    for (int n1 = 0; n1 < C::P; n1++) srow[C::Q * n1 + n2] = x[n1];
+    ts_f2_fence_async();
+  }
+  __syncthreads();
+  if (tid < C::R) {
+    const int lat = lat_of(tid);
+    if (lat >= 0) {
+      ts_f2_bulk_s2g(dst + (long)lat * nphi, b + tid * C::H, (unsigned)(nphi * sizeof(float)));
+      ts_f2_bulk_commit();
+      ts_f2_bulk_wait_read();
+    }
+  }
+}
+
 // ts_f2_forward whose first phase reads z straight from the grid rows
 template <class C, class LatOf>
 TS_DEV void ts_f2_forward_in(float2 *b, const float2 *twq, const float *__restrict__ src, int nphi,
@@ -537,13 +598,14 @@ constexpr long ts_f2_smem_bytes(int nb) {
 #define TS_F2_PHASE_MINB(P, R) 1
 
 // fm[field][m][lat] -> spat[field][lat][phi].  grid = (ceil(nlat/R), fields),
-// block = P*R.
+// block = P*R.  Rows leave by bulk copies when the field's grid is 16-byte
+// aligned (fewer, larger memory instructions), else by per-thread stores.
 template <int P, int Q, int R>
 __global__ void __launch_bounds__(P *R, TS_F2_MINB(P, R))
 ts_f2_synth(TsFftTab ft, const float2 *__restrict__ fm, long fm_stride, float *__restrict__ spat,
             long spat_stride) {
   using C = TsF2<P, Q, R>;
-  extern __shared__ float2 ts_smem_f2s[];
+  extern __shared__ __align__(16) float2 ts_smem_f2s[];
   float2 *twq = ts_smem_f2s;
   float2 *b = twq + C::TWQ;
   const long f = blockIdx.y;
@@ -551,7 +613,12 @@ ts_f2_synth(TsFftTab ft, const float2 *__restrict__ fm, long fm_stride, float *_
   ts_f2_twq<C>(twq, ft);
   ts_f2_pack<C>(b, fm + f * fm_stride, ft, rows);
   __syncthreads();
-  ts_f2_inverse_out<C>(b, twq, spat + f * spat_stride, ft.nphi, rows);
+  float *dst = spat + f * spat_stride;
+  if ((reinterpret_cast<unsigned long long>(dst) & 15) == 0 && (ft.nphi & 3) == 0 &&
+      (C::H & 1) == 0 && ((C::TWQ * sizeof(float2)) & 15) == 0)
+    ts_f2_inverse_bulk<C>(b, twq, dst, ft.nphi, rows);
+  else
+    ts_f2_inverse_out<C>(b, twq, dst, ft.nphi, rows);
 }
 
 // spat[field][lat][phi] -> g[field][m][lat].  grid = (ceil(nlat/R), fields).
