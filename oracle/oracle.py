@@ -59,6 +59,11 @@ def _load():
     lib.ors_model_species.argtypes = [C.c_int]
     lib.ors_model_step.restype = C.c_int
     lib.ors_model_step.argtypes = [C.c_void_p, C.c_int, _d, _d, C.c_int, C.c_int]
+    lib.ors_synth_adjoint.argtypes = [C.c_void_p, _d, _d, C.c_int]
+    lib.ors_analys_adjoint.argtypes = [C.c_void_p, _d, _d, C.c_int]
+    lib.ors_model_adjoint.restype = C.c_int
+    lib.ors_model_adjoint.argtypes = [C.c_void_p, C.c_int, _d, _d, C.c_int, C.c_int, _d, _d, _d,
+                                      C.c_int]
     return lib
 
 
@@ -170,18 +175,12 @@ class ShtReference:
 
     def synth_adjoint(self, gbar):
         """S^T gbar, the transpose of synth with coefficients read as 2*nlm
-        reals: c_m * analys(gbar / (w_i 2 pi/nphi)), c_0 = 1, c_m = 2 (a real
-        field from its m >= 0 half), m = 0 imaginary parts zero.  Test
-        helper for the adjoint's losses."""
-        g = np.asarray(gbar, dtype=np.float64).reshape(self.nlat, self.nphi)
-        q = self.analys((g / (self.wg[:, None] * (2 * np.pi / self.nphi))).ravel())
-        if not hasattr(self, "_c"):
-            c = np.full(2 * self.nlm, 2.0)
-            for l in range(self.lmax + 1):
-                i = lm_index(self.lmax, l, 0)
-                c[2 * i], c[2 * i + 1] = 1.0, 0.0
-            self._c = c
-        return q * self._c
+        reals (m = 0 imaginary parts zero)."""
+        return self._run("ors_synth_adjoint", gbar, 2 * self.nlm)
+
+    def analys_adjoint(self, qbar):
+        """A^T qbar, the transpose of analys (spectral cotangent -> grid)."""
+        return self._run("ors_analys_adjoint", qbar, self.nlat * self.nphi)
 
     def model_step(self, model: str, params, state, nsteps: int):
         """Advance ``state`` (species x 2*nlm, f64) by ``nsteps`` IMEX steps."""
@@ -193,6 +192,23 @@ class ShtReference:
         if rc != 0:
             raise ValueError(f"unknown model {model}")
         return st
+
+    def model_adjoint(self, model: str, params, state, nsteps: int, every: int, final_bar):
+        """Reverse mode of ``nsteps`` model steps from ``state`` (species x
+        2*nlm) with checkpoints every ``every`` steps: returns
+        (dL/d state, dL/d params) for dL/d(final state) = ``final_bar``."""
+        mid = MODELS[model]
+        S = int(_lib.ors_model_species(mid))
+        st = np.ascontiguousarray(np.array(state, dtype=np.float64).reshape(S, 2 * self.nlm))
+        fb = np.ascontiguousarray(np.array(final_bar, dtype=np.float64).reshape(S, 2 * self.nlm))
+        prm = np.ascontiguousarray(np.array(params, dtype=np.float64))
+        ib = np.zeros_like(st)
+        pb = np.zeros(prm.size)
+        rc = _lib.ors_model_adjoint(self._p, mid, prm, st, nsteps, every, fb, ib, pb,
+                                    self.threads)
+        if rc != 0:
+            raise ValueError(f"unknown model {model}")
+        return ib, pb
 
 
 def rel_l2(a, b) -> float:

@@ -202,9 +202,11 @@ void ors_plan_nodes(const ors_plan *p, double *ct, double *wg) {
   memcpy(wg, p->wg, sizeof(double) * p->nlat);
 }
 
+/* threads > 0: that many OpenMP threads; 0: every host core (set each call,
+ * so a single-threaded call does not leave later calls on one thread). */
 static void ors_set_threads(int threads) {
 #ifdef _OPENMP
-  if (threads > 0) omp_set_num_threads(threads);
+  omp_set_num_threads(threads > 0 ? threads : omp_get_num_procs());
 #else
   (void)threads;
 #endif
@@ -498,5 +500,213 @@ int ors_model_step(const ors_plan *p, int model, const double *prm, double *stat
   free(grid);
   free(rgrid);
   free(rq);
+  return 0;
+}
+
+/* ---------------------------------------------------------------- adjoint
+ *
+ * The reference has no differentiation.  These are the f64 transposes of this
+ * file's own forward step, the check for a GPU adjoint: each function is the
+ * exact adjoint (transpose) of the f64 map above it applies to.
+ *
+ * Transforms.  Reading coefficients as 2*nlm reals and the grid as
+ * nlat*nphi reals, ors_synth is S and ors_analys is A with
+ *   S[(i,j),(l,m,re)] =  c_m P_lm(x_i) cos(m phi_j),
+ *   S[(i,j),(l,m,im)] = -c_m P_lm(x_i) sin(m phi_j),
+ *   A[(l,m,.),(i,j)]  = w'_i S[(i,j),(l,m,.)] / c_m,
+ * c_0 = 1, c_m = 2 (m >= 1), w'_i = w_i 2 pi/nphi (the Gauss weight times
+ * the longitude quadrature weight).  Hence S^T = C A W'^-1 and
+ * A^T = W' S C^-1; the m = 0 imaginary entries are zero rows of A and zero
+ * columns of S, so both adjoints leave them zero. */
+
+static double ors_cm(int lmax, long lm) {
+  /* m of coefficient lm: m = 0 occupies lm = 0..lmax */
+  return lm <= lmax ? 1.0 : 2.0;
+}
+
+/* qbar = S^T gbar */
+void ors_synth_adjoint(const ors_plan *p, const double *gbar, double *qbar, int threads) {
+  const long npts = (long)p->nlat * p->nphi;
+  double *g = (double *)malloc(sizeof(double) * npts);
+  const double lon = 2.0 * M_PI / p->nphi;
+  for (int i = 0; i < p->nlat; i++)
+    for (int j = 0; j < p->nphi; j++) {
+      long o = (long)i * p->nphi + j;
+      g[o] = gbar[o] / (p->wg[i] * lon);
+    }
+  ors_analys(p, g, qbar, threads);
+  for (long lm = 0; lm < p->nlm; lm++) {
+    double c = ors_cm(p->lmax, lm);
+    qbar[2 * lm] *= c;
+    qbar[2 * lm + 1] = lm <= p->lmax ? 0.0 : qbar[2 * lm + 1] * c;
+  }
+  free(g);
+}
+
+/* gbar = A^T qbar */
+void ors_analys_adjoint(const ors_plan *p, const double *qbar, double *gbar, int threads) {
+  double *q = (double *)malloc(sizeof(double) * 2 * p->nlm);
+  for (long lm = 0; lm < p->nlm; lm++) {
+    double c = ors_cm(p->lmax, lm);
+    q[2 * lm] = qbar[2 * lm] / c;
+    q[2 * lm + 1] = lm <= p->lmax ? 0.0 : qbar[2 * lm + 1] / c;
+  }
+  ors_synth(p, q, gbar, threads);
+  const double lon = 2.0 * M_PI / p->nphi;
+  for (int i = 0; i < p->nlat; i++)
+    for (int j = 0; j < p->nphi; j++) gbar[(long)i * p->nphi + j] *= p->wg[i] * lon;
+  free(q);
+}
+
+/* Pointwise vector-Jacobian product of the reaction of ors_react: given the
+ * cotangents (r1b, r2b) of its outputs at one grid point, accumulate the
+ * cotangents of its inputs (u, v) and of its parameters (pb, in the model's
+ * parameter order). */
+static void ors_react_vjp(int model, const double *prm, double u, double v, double r1b,
+                          double r2b, double *ub, double *vb, double *pb) {
+  switch (model) {
+    case 0: /* r1 = a - u + u^2 v, r2 = b - u^2 v */
+      *ub = (-1.0 + 2.0 * u * v) * r1b - 2.0 * u * v * r2b;
+      *vb = u * u * (r1b - r2b);
+      pb[0] += r1b;
+      pb[1] += r2b;
+      break;
+    case 1: /* r1 = A - (B+1) u + u^2 v, r2 = B u - u^2 v */
+      *ub = (-(prm[1] + 1.0) + 2.0 * u * v) * r1b + (prm[1] - 2.0 * u * v) * r2b;
+      *vb = u * u * (r1b - r2b);
+      pb[0] += r1b;
+      pb[1] += u * (r2b - r1b);
+      break;
+    case 2: /* r = u - u^3 */
+      *ub = (1.0 - 3.0 * u * u) * r1b;
+      break;
+    case 3: /* r = c u */
+      *ub = prm[0] * r1b;
+      pb[0] += u * r1b;
+      break;
+    case 4: /* r = r u (1 - u) */
+      *ub = prm[0] * (1.0 - 2.0 * u) * r1b;
+      pb[0] += u * (1.0 - u) * r1b;
+      break;
+  }
+}
+
+/* parameter indices of dt and of the diffusion coefficient of each species */
+static int ors_imex_indices(int model, int *idt, int *iD) {
+  switch (model) {
+    case 0:
+    case 1:
+      *idt = 4;
+      iD[0] = 2;
+      iD[1] = 3;
+      return 2;
+    case 2:
+      *idt = 1;
+      iD[0] = 0;
+      return 0;
+    case 3:
+    case 4:
+      *idt = 2;
+      iD[0] = 1;
+      return 0;
+  }
+  return -1;
+}
+
+/* Reverse mode of `nsteps` steps of ors_model_step from state0 (S x 2 nlm):
+ * given final_bar = dL/d(final state), writes init_bar = dL/d(state0) and
+ * param_bar = dL/d(params) (the model's parameter order; dt and the
+ * diffusion coefficients include their appearance in the implicit solve).
+ * States are kept every `every` steps and each segment is recomputed from its
+ * checkpoint before it is reversed.  Per step, with d = 1/(1 + dt D lam),
+ * U' = (U + dt R) d:
+ *   dL/dU += d Ubar',   Rbar = dt d Ubar',   rbar = A^T Rbar (grid),
+ *   (ubar, vbar, pbar) += reaction VJP of rbar,  dL/dU += S^T ubar,
+ *   dL/d dt += sum d Ubar' (R - D lam U'),  dL/dD += sum -dt lam d U' Ubar'. */
+int ors_model_adjoint(const ors_plan *p, int model, const double *prm, const double *state0,
+                      int nsteps, int every, const double *final_bar, double *init_bar,
+                      double *param_bar, int threads) {
+  int idt, iD[2] = {0, 0};
+  if (ors_imex_indices(model, &idt, iD) < 0) return -1;
+  if (every < 1) every = 1;
+  const int S = ors_model_species(model);
+  const long n2 = 2 * p->nlm, npts = (long)p->nlat * p->nphi;
+  const int nprm = model <= 1 ? 5 : (model == 2 ? 2 : 3);
+  const double dt = prm[idt];
+  const int nck = (nsteps + every - 1) / every;
+  double *ck = (double *)malloc(sizeof(double) * (nck + 1) * S * n2);
+  double *seg = (double *)malloc(sizeof(double) * (every + 1) * S * n2);
+  double *lam = (double *)malloc(sizeof(double) * n2);
+  double *grid = (double *)malloc(sizeof(double) * S * npts);
+  double *rgrid = (double *)malloc(sizeof(double) * S * npts);
+  double *gbar = (double *)malloc(sizeof(double) * S * npts);
+  double *rq = (double *)malloc(sizeof(double) * S * n2);
+  double *xbar = (double *)malloc(sizeof(double) * S * n2);
+  double *nbar = (double *)malloc(sizeof(double) * S * n2);
+  double *tmp = (double *)malloc(sizeof(double) * n2);
+  ors_eigenvalues(p->lmax, p->mmax, lam);
+  /* forward: checkpoints at steps 0, every, 2 every, ... */
+  memcpy(ck, state0, sizeof(double) * S * n2);
+  for (int c = 1; c <= nck; c++) {
+    memcpy(ck + (long)c * S * n2, ck + (long)(c - 1) * S * n2, sizeof(double) * S * n2);
+    int len = (c * every <= nsteps) ? every : nsteps - (c - 1) * every;
+    ors_model_step(p, model, prm, ck + (long)c * S * n2, len, threads);
+  }
+  memcpy(xbar, final_bar, sizeof(double) * S * n2);
+  for (int k = 0; k < nprm; k++) param_bar[k] = 0.0;
+  for (int c = nck - 1; c >= 0; c--) {
+    const int len = ((c + 1) * every <= nsteps) ? every : nsteps - c * every;
+    memcpy(seg, ck + (long)c * S * n2, sizeof(double) * S * n2);
+    for (int t = 1; t <= len; t++) {
+      memcpy(seg + (long)t * S * n2, seg + (long)(t - 1) * S * n2, sizeof(double) * S * n2);
+      ors_model_step(p, model, prm, seg + (long)t * S * n2, 1, threads);
+    }
+    for (int t = len - 1; t >= 0; t--) {
+      const double *U = seg + (long)t * S * n2, *Un = seg + (long)(t + 1) * S * n2;
+      for (int k = 0; k < S; k++) ors_synth(p, U + k * n2, grid + k * npts, threads);
+      for (long i = 0; i < npts; i++) {
+        double r1 = 0, r2 = 0;
+        ors_react(model, prm, grid[i], S > 1 ? grid[npts + i] : 0.0, &r1, &r2);
+        rgrid[i] = r1;
+        if (S > 1) rgrid[npts + i] = r2;
+      }
+      for (int k = 0; k < S; k++) {
+        ors_analys(p, rgrid + k * npts, rq + k * n2, threads);
+        const double D = prm[iD[k]];
+        for (long i = 0; i < n2; i++) {
+          const double d = 1.0 / (1.0 + dt * D * lam[i]);
+          const double ub = xbar[k * n2 + i];
+          param_bar[idt] += ub * d * (rq[k * n2 + i] - D * lam[i] * Un[k * n2 + i]);
+          param_bar[iD[k]] += -ub * dt * lam[i] * d * Un[k * n2 + i];
+          nbar[k * n2 + i] = ub * d;
+          tmp[i] = dt * ub * d;
+        }
+        ors_analys_adjoint(p, tmp, rgrid + k * npts, threads); /* rgrid now holds rbar */
+      }
+      for (long i = 0; i < npts; i++) {
+        double ub = 0, vb = 0;
+        ors_react_vjp(model, prm, grid[i], S > 1 ? grid[npts + i] : 0.0, rgrid[i],
+                      S > 1 ? rgrid[npts + i] : 0.0, &ub, &vb, param_bar);
+        gbar[i] = ub;
+        if (S > 1) gbar[npts + i] = vb;
+      }
+      for (int k = 0; k < S; k++) {
+        ors_synth_adjoint(p, gbar + k * npts, tmp, threads);
+        for (long i = 0; i < n2; i++) nbar[k * n2 + i] += tmp[i];
+      }
+      memcpy(xbar, nbar, sizeof(double) * S * n2);
+    }
+  }
+  memcpy(init_bar, xbar, sizeof(double) * S * n2);
+  free(ck);
+  free(seg);
+  free(lam);
+  free(grid);
+  free(rgrid);
+  free(gbar);
+  free(rq);
+  free(xbar);
+  free(nbar);
+  free(tmp);
   return 0;
 }

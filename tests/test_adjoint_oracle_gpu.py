@@ -1,0 +1,85 @@
+"""The GPU's hand-written adjoint against the oracle's f64 CPU adjoint (the
+reverse mode of the f64 IMEX steps, itself pinned to finite differences in
+tests/test_oracle_adjoint.py), on identical initial states and cotangents of
+the final state, through the C ABI.  Bar: 1e-4 relative (L2 over the
+initial-state gradient and over the parameter-gradient vector)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.test_adjoint_gpu import spectrum_l2
+from tests.test_model_gpu import spectral_seed
+from turing_sphere_b200 import (GpuModel, ShtConfig, ShtPlan, defaultParams, mModelByKey)
+
+pytestmark = pytest.mark.gpu
+
+BAR = 1e-4
+
+
+def test_schnakenberg_sweep_200_steps_matches_f64_adjoint(device, parity):
+    """Two Schnakenberg instances (own a, D1) at lmax 63 on 96 x 192,
+    tensor-core plan, 200 steps with checkpoints every 32; L = sum <w, final
+    state>: gradients w.r.t. the initial (U, V) and (a, b, D1, D2, dt)."""
+    model = mModelByKey("schnakenberg")
+    lmax, nlat, nphi, nsteps, every = 63, 96, 192, 200, 32
+    base = defaultParams(model)
+    names = [q.key for q in model.params]
+    sweep = [dict(base, a=base["a"] + 0.02 * k, D1=base["D1"] * (1 + 0.5 * k)) for k in range(2)]
+    sht = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi), {"precision": "tf32x3"})
+    gpu = GpuModel.create(device, sht, model.source, names, list(model.state),
+                          list(model.species), 2)
+    gpu.setParams(sweep)
+    x0 = [np.stack(spectral_seed(lmax, sweep[k], 1 + k)) for k in range(2)]
+    gpu.upload("U", np.stack([x[0] for x in x0]))
+    gpu.upload("V", np.stack([x[1] for x in x0]))
+    w = np.random.default_rng(4).standard_normal((2, 2, 2 * sht.nlm)).astype(np.float32)
+    init_bar, pbar = gpu.forwardBackward(nsteps, every, {"U": w[:, 0], "V": w[:, 1]})
+    gpu.destroy()
+    sht.destroy()
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    for k in range(2):
+        prm = [sweep[k][n] for n in names]
+        ib, pb = ref.model_adjoint("schnakenberg", prm, x0[k].astype(np.float64), nsteps, every,
+                                   w[k].astype(np.float64))
+        got = np.stack([init_bar["U"][k], init_bar["V"][k]])
+        parity(f"adjoint schnakenberg lmax63 200 steps inst{k} d/dstate0", O.rel_l2(got, ib), BAR)
+        parity(f"adjoint schnakenberg lmax63 200 steps inst{k} d/dparams",
+               O.rel_l2(pbar[k], pb), BAR)
+        # per component: |d/da| is ~1e-3 of the vector's norm here, so its
+        # own relative error carries the vector's absolute error (measured
+        # up to ~2e-4); each component is held to the bar relative to the norm
+        for j, n in enumerate(names):
+            assert abs(pbar[k, j] - pb[j]) <= BAR * np.linalg.norm(pb), (k, n, pbar[k, j], pb[j])
+
+
+def test_allencahn_lmax255_matches_f64_adjoint(device, parity):
+    """The Allen-Cahn adjoint workload's grid (lmax 255, 384 x 768),
+    tensor-core plan, initial coefficients with an l^-2 spectrum, 64 steps
+    with checkpoints every 32; L = ||u(T) - u_target||^2 on the grid:
+    gradients w.r.t. the initial coefficients and (eps2, dt)."""
+    model = mModelByKey("allencahn")
+    lmax, nlat, nphi, nsteps, every = 255, 384, 768, 64, 32
+    p = defaultParams(model)
+    prm = [p["eps2"], p["dt"]]
+    sht = ShtPlan.create(device, ShtConfig(lmax, lmax, nlat, nphi), {"precision": "tf32x3"})
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    U0 = spectrum_l2(lmax, 1, amp=0.5, base=0.1)
+    target = ref.synth(spectrum_l2(lmax, 2, amp=0.5, base=-0.1))
+    gpu = GpuModel.create(device, sht, model.source, ["eps2", "dt"], ["U"], ["u"], 1)
+    gpu.setParams(p)
+    gpu.upload("U", U0.astype(np.float32))
+    fbar = {}
+
+    def final_bar(final):
+        u = ref.synth(final["U"][0].astype(np.float64))
+        fbar["U"] = ref.synth_adjoint(2.0 * (u - target))
+        return {"U": fbar["U"][None, :]}
+
+    init_bar, pbar = gpu.lossGradient(nsteps, every, final_bar)
+    gpu.destroy()
+    sht.destroy()
+    ib, pb = ref.model_adjoint("allencahn", prm, U0[None, :], nsteps, every, fbar["U"][None, :])
+    parity("adjoint allencahn lmax255 64 steps d/dU0", O.rel_l2(init_bar["U"][0], ib[0]), BAR)
+    for j, n in enumerate(("eps2", "dt")):
+        parity(f"adjoint allencahn lmax255 64 steps d/d{n}", abs(pbar[0, j] - pb[j]) / abs(pb[j]),
+               BAR)
