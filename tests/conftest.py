@@ -29,3 +29,26 @@ def device():
         pytest.skip("no CUDA device")
     from turing_sphere_b200 import requestShtDevice
     return requestShtDevice(0)
+
+
+# relative L2 errors measured by the parity tests, printed at the end of the run
+_PARITY = []
+
+
+@pytest.fixture
+def parity():
+    """parity(name, err, bound): records a measured relative L2 error against
+    the f64 oracle, asserts it is within `bound`, and returns it."""
+    def record(name, err, bound):
+        _PARITY.append((name, float(err), float(bound)))
+        assert err <= bound, (name, err, bound)
+        return err
+    return record
+
+
+def pytest_terminal_summary(terminalreporter):
+    if not _PARITY:
+        return
+    terminalreporter.write_line("relL2 vs the f64 oracle (measured <= bound):")
+    for name, err, bound in _PARITY:
+        terminalreporter.write_line(f"  {name}: {err:.2e} <= {bound:.0e}")

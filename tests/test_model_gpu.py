@@ -162,13 +162,9 @@ def spectral_seed(lmax, p, seed, amp=1e-2):
     out = []
     for base in (us, vs):
         q = (amp * rng.standard_normal(2 * nlm)).astype(np.float32)
-        for m in range(lmax + 1):
-            for l in range(m, lmax + 1):
-                i = lmIndex(lmax, l, m)
-                if l == 0:
-                    q[2 * i] = base * math.sqrt(4 * math.pi)
-                if m == 0:
-                    q[2 * i + 1] = 0.0
+        # m = 0 comes first in m-major order: lm(l, 0) = l, so (l, m) = (0, 0) is lm 0
+        q[0] = base * math.sqrt(4 * math.pi)
+        q[1:2 * (lmax + 1):2] = 0.0
         out.append(q)
     return out
 

@@ -83,3 +83,89 @@ def test_two_rank_sweep_equals_serial(tmp_path):
     assert full.shape[0] == N
     np.testing.assert_array_equal(full, run_instances(range(N)))
     assert float(np.load(out + ".max.npy")[0]) == 2.0
+
+
+# ------------------------------------------------ the library, sharded (GPU)
+GPU_LMAX, GPU_STEPS = 31, 20
+
+
+def gpu_sweep(k):
+    from turing_sphere_b200 import defaultParams, mModelByKey
+    p = defaultParams(mModelByKey("schnakenberg"))
+    return dict(p, b=p["b"] + 0.02 * k)
+
+
+def gpu_run(ks):
+    """Schnakenberg instances ks through the library (one batched model on a
+    tensor-core plan), spectral seed 1 + k; returns their U states."""
+    from tests.test_model_gpu import spectral_seed
+    from turing_sphere_b200 import ModelSession, mModelByKey, requestShtDevice
+    dev = requestShtDevice(0)
+    model = mModelByKey("schnakenberg")
+    sweep = [gpu_sweep(k) for k in ks]
+    s = ModelSession.create(dev, model, sweep, GPU_LMAX, batch=len(ks), precision="tf32x3")
+    seeds = [spectral_seed(GPU_LMAX, sweep[i], 1 + k) for i, k in enumerate(ks)]
+    s.gpu.upload("U", np.stack([q[0] for q in seeds]))
+    s.gpu.upload("V", np.stack([q[1] for q in seeds]))
+    s.step(GPU_STEPS)
+    U = s.read("U").reshape(len(ks), -1)
+    s.destroy()
+    return U
+
+
+def gpu_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    import torch.distributed as dist
+    from turing_sphere_b200.shard import gather_instances
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        start, count = shard_range(N, rank, world)
+        full = gather_instances(gpu_run(list(range(start, start + count))), N)
+        if rank == 0:
+            np.save(out, full)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_two_rank_library_sweep_equals_unsharded(tmp_path):
+    """The sharded path of the library itself: two ranks (gloo for the gather;
+    both on GPU 0, each with its own CUDA context and its own block of a
+    5-instance Schnakenberg sweep, no kernel waiting on the other rank) run
+    their blocks through the C ABI; the gathered states match the f64 oracle
+    stepping each instance alone, and the unsharded batch run in this
+    process, instance by instance."""
+    from tests.conftest import HAS_GPU
+    if not HAS_GPU:
+        pytest.skip("no CUDA device")
+    from oracle import oracle as O
+    from tests.test_model_gpu import spectral_seed
+    from turing_sphere_b200 import gridForLmax
+    out = str(tmp_path / "gathered_gpu.npy")
+    ctx = mp.get_context("spawn")
+    port = free_port()
+    procs = [ctx.Process(target=gpu_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    full = np.load(out)
+    nlat, nphi = gridForLmax(GPU_LMAX, 3)
+    ref = O.ShtReference(GPU_LMAX, GPU_LMAX, nlat, nphi)
+    want = []
+    for k in range(N):
+        p = gpu_sweep(k)
+        st = np.stack(spectral_seed(GPU_LMAX, p, 1 + k)).astype(np.float64)
+        want.append(ref.model_step("schnakenberg", [p[n] for n in ("a", "b", "D1", "D2", "dt")],
+                                   st, GPU_STEPS)[0])
+    here = gpu_run(list(range(N)))
+    assert full.shape == here.shape
+    e_sharded = [O.rel_l2(full[k], want[k]) for k in range(N)]
+    e_here = [O.rel_l2(here[k], want[k]) for k in range(N)]
+    assert max(e_sharded) < 1e-5 and max(e_here) < 1e-5, (e_sharded, e_here)
+    for k in range(N):
+        assert O.rel_l2(full[k], here[k]) < 1e-6, k

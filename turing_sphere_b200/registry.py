@@ -96,3 +96,23 @@ presets = [
     Preset("brussel", "Brusselator - stripes & spots", "brusselator"),
     Preset("allencahn", "Allen-Cahn - coarsening", "allencahn"),
 ]
+
+
+def brusselatorSweep(n: int, seed: int = 3, base: dict | None = None) -> list:
+    """Parameter sets for a Brusselator sweep over its Turing-unstable band:
+    A ~ U[2.5, 3.5], then B ~ U between the Turing threshold
+    (1 + A sqrt(D1/D2))^2 and the Hopf bound 1 + A^2, with D1, D2 and dt the
+    model's defaults (brusselator.m:22-28; registry.ts:79-83 of the
+    reference).  Deterministic for a given seed."""
+    import math
+
+    import numpy as np
+
+    p = dict(base or defaultParams(brusselator))
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        a = float(rng.uniform(2.5, 3.5))
+        lo = (1 + a * math.sqrt(p["D1"] / p["D2"])) ** 2
+        out.append(dict(p, A=a, B=float(rng.uniform(lo, 1 + a * a))))
+    return out
