@@ -16,6 +16,11 @@
  *   - `_dev` entry points take device pointers and a cudaStream_t passed as
  *     void* (NULL = the context's stream) and return without synchronising;
  *     the others take caller-owned HOST arrays and block until done;
+ *   - device arrays of the transforms must be 8-byte aligned (coefficient
+ *     pairs and grid rows are accessed as float2): other pointers are refused
+ *     with TS_ERR_INVALID before anything runs;
+ *   - every call makes the context's device current for its duration and
+ *     gives the calling thread back the CUDA context it had on entry;
  *   - one host thread per context.
  *
  * Layouts (src/sht/layout.ts:1-16): spectral arrays are float pairs
@@ -159,11 +164,24 @@ int ts_sht_analys_dev(ts_plan plan, const float *spat, float *qlm, int batch, vo
 int ts_sht_synth_noalloc(ts_plan plan, const float *qlm, float *spat, int batch, void *stream);
 
 /* Blocking transforms on host arrays (ShtPlan.synth / ShtPlan.analys,
- * sht.ts:414-461); they fail with TS_ERR_SIZE on a length mismatch. */
+ * sht.ts:414-461); they fail with TS_ERR_SIZE on a length mismatch.  A batch
+ * moves in chunks of fields: one chunk's host->device copy, another's
+ * transform and a third's device->host copy run at once (two copy streams
+ * and the context's stream, ordered by events).  Page-locked host arrays
+ * (cudaHostAlloc / cudaHostRegister) get the full overlap; pageable arrays
+ * are correct but copied through the driver's staging.  Staging device
+ * arrays are plan-owned and grown on first use. */
 int ts_sht_synth(ts_plan plan, const float *qlm, long qlm_len, float *spat, long spat_len,
                  int batch);
 int ts_sht_analys(ts_plan plan, const float *spat, long spat_len, float *qlm, long qlm_len,
                   int batch);
+/* Round trips on host arrays: qlm_out = analys(synth(qlm_in)) per field, the
+ * grid staying on the device.  The round trip of scripts/bench-sht.ts:190-217
+ * (coefficients written to the device, encodeSynthInto + encodeAnalysInto,
+ * the result copied to a readback buffer and mapped) as one blocking call,
+ * pipelined over chunks of fields like ts_sht_synth. */
+int ts_sht_roundtrip(ts_plan plan, const float *qlm_in, long in_len, float *qlm_out,
+                     long out_len, int batch);
 
 /* Single stages, for diagnostics (ShtPlan.encodeStage, sht.ts:362-401;
  * scripts/diagnose-sht.ts).  fm is [B][mmax+1][nlat] complex (2 floats). */

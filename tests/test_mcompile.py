@@ -151,3 +151,20 @@ def test_comments_and_continuations():
     src = LINEAR.replace("Un = (U + dt * analys(c * u))",
                          "%{\nblock comment\n%}\n  Un = (U + dt * ... continued\n analys(c * u))")
     check(src, params=["c", "D", "dt"])
+
+
+def test_round_rounds_halfway_cases_to_even():
+    """WGSL round (src/mgpu/wgsl.ts:64 maps .m round to it) takes a halfway
+    value to the even integer; the generated CUDA calls rintf (round to
+    nearest even), not roundf (halfway cases away from zero)."""
+    src = LINEAR.replace("analys(c * u)", "analys(c * round(u))")
+    buf = C.create_string_buffer(1 << 20)
+    k, n = C.c_int(), C.c_int()
+    err = _lib.CompileError()
+    rc = _lib.lib().ts_model_check(15, 15, 16, 32, src.encode(), _lib.cstr_array(["U"]), 1,
+                                   _lib.cstr_array(["u"]), 1, _lib.cstr_array(["c", "D", "dt"]),
+                                   3, 1, _lib.TS_CHECK_SOURCE, buf, len(buf), C.byref(k),
+                                   C.byref(n), C.byref(err))
+    assert rc == _lib.TS_OK, err.message.decode()
+    code = buf.value.decode()
+    assert "rintf(" in code and "roundf(" not in code

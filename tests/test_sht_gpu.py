@@ -202,6 +202,78 @@ def test_device_pointer_batch(device):
     assert O.rel_l2(qo.cpu().numpy(), qs) < TOL
 
 
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
+@pytest.mark.parametrize("pinned", [False, True], ids=["pageable", "pinned"])
+def test_host_array_transforms_in_chunks(device, precision, pinned, monkeypatch):
+    """ts_sht_synth / ts_sht_analys / ts_sht_roundtrip on host arrays, moved
+    in chunks of 5 fields (5 + 5 + 3: copies of one chunk overlap the
+    transform of another): every field against the f64 oracle, and the round
+    trip equal to analys(synth) of the separate calls.  Pageable numpy arrays
+    and page-locked ones."""
+    import torch
+    monkeypatch.setenv("TS_HOST_CHUNK", "5")
+    lmax, (nlat, nphi) = 63, gaussGrid(63)
+    plan = make(device, lmax, nlat, nphi, precision=precision)
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    B, n2 = 13, 2 * plan.nlm
+
+    def host(n):
+        if pinned:
+            return torch.empty(n, dtype=torch.float32).pin_memory().numpy()
+        return np.empty(n, dtype=np.float32)
+
+    qs = host(B * n2)
+    qs[:] = np.stack([scaled_spectrum(lmax, lmax, 60 + b) for b in range(B)]).ravel()
+    spat = plan.synth(qs, batch=B).reshape(B, -1)
+    for b in (0, 6, 12):
+        assert O.rel_l2(spat[b], ref.synth(qs[b * n2:(b + 1) * n2].astype(np.float64))) < TOL
+    sp = host(spat.size)
+    sp[:] = spat.ravel()
+    back = plan.analys(sp, batch=B).reshape(B, -1)
+    for b in (0, 6, 12):
+        want = ref.analys(spat[b].astype(np.float64))
+        assert O.rel_l2(back[b], want) < TOL
+    rt = plan.roundtrip(qs, batch=B, out=host(B * n2)).reshape(B, -1)
+    assert O.rel_l2(rt, back) < 1e-6
+    assert O.rel_l2(rt, qs.reshape(B, -1)) < TOL
+    with pytest.raises(Exception, match="qlm_in must have length"):
+        plan.roundtrip(qs[:-2], batch=B)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
+def test_grids_aligned_to_8_but_not_16_bytes(device, precision):
+    """Grid arrays that start 8 bytes past a 16-byte boundary: the Fourier
+    synthesis then writes rows with per-thread float2 stores instead of bulk
+    copies, and the analysis reads them back; both stay within the transform
+    bar of the f64 oracle.  A 4-byte-aligned pointer (legal for float*, but
+    not for the float2 rows the kernels access) is refused before any
+    launch."""
+    import torch
+    from turing_sphere_b200 import _lib
+    lmax, (nlat, nphi) = 127, gaussGrid(127)
+    plan = make(device, lmax, nlat, nphi, precision=precision)
+    B, npts = 3, nlat * nphi
+    qs = np.stack([scaled_spectrum(lmax, lmax, 40 + b) for b in range(B)])
+    qd = torch.from_numpy(qs).cuda()
+    qo = torch.empty_like(qd)
+    raw = torch.empty(B * npts + 4, device="cuda")
+    spat = raw[2:2 + B * npts]
+    assert spat.data_ptr() % 16 == 8
+    plan.synth_dev(qd.data_ptr(), spat.data_ptr(), B)
+    plan.analys_dev(spat.data_ptr(), qo.data_ptr(), B)
+    device.sync()
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    got = spat.view(B, npts).cpu().numpy()
+    for b in (0, B - 1):
+        assert O.rel_l2(got[b], ref.synth(qs[b].astype(np.float64))) < TOL
+    assert O.rel_l2(qo.cpu().numpy(), qs) < TOL
+    odd = raw[1:1 + B * npts]
+    for fn, a, b in (("ts_sht_synth_dev", qd, odd), ("ts_sht_analys_dev", odd, qo)):
+        rc = getattr(_lib.lib(), fn)(plan.handle, a.data_ptr(), b.data_ptr(), B, None)
+        assert rc == _lib.TS_ERR_INVALID
+        assert b"8-byte aligned" in _lib.lib().ts_last_error(device.handle)
+
+
 def test_errors(device):
     plan = make(device, 31, 32, 64)
     with pytest.raises(ValueError, match="qlm must have length"):
@@ -243,3 +315,22 @@ def test_transform_adjoints_dot_product(device, precision, lmax, nlat, nphi):
     # m = 0 imaginary parts of the spectral cotangent are zero
     idx = [2 * i + 1 for i in range(lmax + 1)]  # m = 0 block, imaginary
     assert float(STg[:, idx].abs().max()) == 0.0
+
+
+def test_second_device_in_the_same_process(device):
+    """A context on a second GPU of the process gets its own kernel attributes
+    (shared-memory limits are set per device): the FP32 path at lmax 1023
+    needs ~73 KB of dynamic shared memory in the synthesis and must launch
+    there too.  Skipped when only one GPU is visible."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one GPU visible")
+    from turing_sphere_b200 import Device
+    dev1 = Device(1)
+    lmax, nlat, nphi = 1023, 1536, 3072
+    plan = ShtPlan.create(dev1, ShtConfig(lmax, lmax, nlat, nphi))
+    q = scaled_spectrum(lmax, lmax, 3)
+    back = plan.analys(plan.synth(q))
+    assert O.rel_l2(back, q) < 1e-3
+    plan.destroy()
+    dev1.destroy()

@@ -93,6 +93,7 @@ SIGNATURES = {
     "ts_sht_synth_noalloc": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_synth": (i32, [vp, f32p, i64, f32p, i64, i32]),
     "ts_sht_analys": (i32, [vp, f32p, i64, f32p, i64, i32]),
+    "ts_sht_roundtrip": (i32, [vp, vp, i64, vp, i64, i32]),
     "ts_sht_leg_synth_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_fourier_synth_dev": (i32, [vp, vp, vp, i32, vp]),
     "ts_sht_fourier_analys_dev": (i32, [vp, vp, vp, i32, vp]),

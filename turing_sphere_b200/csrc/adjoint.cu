@@ -104,7 +104,8 @@ int ts_sht_synth_adjoint_dev(ts_plan p, const float *gbar, float *qbar, int batc
     TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
     TS_REQUIRE(gbar != nullptr && qbar != nullptr, TS_ERR_INVALID, "null buffer");
     TS_REQUIRE(batch >= 1 && batch <= 65535, TS_ERR_INVALID, "batch must be in [1, 65535]");
-    TS_CUDA(cudaSetDevice(ctx->device));
+    ts_require_aligned8(gbar, qbar);
+    ts_device_guard dev_guard_(ctx->device);
     ts_synth_adjoint(p, gbar, qbar, batch, ts_pick_stream(ctx, stream));
     return TS_OK;
   } catch (const ts_exc &e) {
@@ -119,7 +120,8 @@ int ts_sht_analys_adjoint_dev(ts_plan p, const float *qbar, float *gbar, int bat
     TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
     TS_REQUIRE(gbar != nullptr && qbar != nullptr, TS_ERR_INVALID, "null buffer");
     TS_REQUIRE(batch >= 1 && batch <= 65535, TS_ERR_INVALID, "batch must be in [1, 65535]");
-    TS_CUDA(cudaSetDevice(ctx->device));
+    ts_require_aligned8(gbar, qbar);
+    ts_device_guard dev_guard_(ctx->device);
     ts_analys_adjoint(p, qbar, gbar, batch, ts_pick_stream(ctx, stream));
     return TS_OK;
   } catch (const ts_exc &e) {

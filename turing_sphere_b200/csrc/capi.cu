@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 
 #include "runtime.h"
@@ -83,6 +84,7 @@ void plan_free(ts_plan p) {
     if (q) cudaFree(q);
   p->fm.release();
   p->stage_q.release();
+  p->stage_q2.release();
   p->stage_s.release();
   p->adj_grid.release();
   p->adj_spec.release();
@@ -93,6 +95,7 @@ void check_batch(ts_plan p, const void *a, const void *b, int batch) {
   TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
   TS_REQUIRE(a != nullptr && b != nullptr, TS_ERR_INVALID, "null buffer");
   TS_REQUIRE(batch >= 1 && batch <= 65535, TS_ERR_INVALID, "batch must be in [1, 65535]");
+  ts_require_aligned8(a, b);
 }
 
 long npts_of(ts_plan p) { return (long)p->nlat * p->nphi; }
@@ -136,6 +139,152 @@ cudaStream_t ts_pick_stream(ts_ctx ctx, void *stream) {
   return stream ? (cudaStream_t)stream : ctx->stream;
 }
 
+namespace {
+using ts_ctx_get_fn = CUresult (*)(CUcontext *);
+using ts_ctx_set_fn = CUresult (*)(CUcontext);
+struct ts_ctx_fns {
+  ts_ctx_get_fn get = nullptr;
+  ts_ctx_set_fn set = nullptr;
+};
+// the driver's current-context calls, through the runtime's entry-point
+// table (the library links the runtime only)
+const ts_ctx_fns &ctx_fns() {
+  static const ts_ctx_fns fns = [] {
+    ts_ctx_fns f;
+    void *g = nullptr, *s = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &g, 12000, cudaEnableDefault, &q1) ==
+            cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess &&
+        cudaGetDriverEntryPointByVersion("cuCtxSetCurrent", &s, 12000, cudaEnableDefault, &q2) ==
+            cudaSuccess &&
+        q2 == cudaDriverEntryPointSuccess) {
+      f.get = (ts_ctx_get_fn)g;
+      f.set = (ts_ctx_set_fn)s;
+    }
+    return f;
+  }();
+  return fns;
+}
+}  // namespace
+
+namespace {
+void check_host_batch(ts_plan p, const void *a, const void *b, int batch) {
+  TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
+  TS_REQUIRE(a != nullptr && b != nullptr, TS_ERR_INVALID, "null buffer");
+  TS_REQUIRE(batch >= 1 && batch <= 65535, TS_ERR_INVALID, "batch must be in [1, 65535]");
+}
+
+void require_len(const char *name, long got, long want) {
+  if (got == want) return;
+  char buf[128];
+  snprintf(buf, sizeof buf, "%s must have length %ld", name, want);
+  ts_throw(TS_ERR_SIZE, buf);
+}
+
+// Fields per chunk of a host-array transform: a quarter of the batch, a
+// multiple of 16 fields, with at most 64 MB of the larger host array per
+// chunk (at lmax 255, 256 fields: 64-field chunks of the round trip's
+// coefficients measured 131 K pairs/s against 126-130 K for 16-32 and
+// 88-117 K for 128-256); a batch under 32 fields moves in one piece.
+// TS_HOST_CHUNK overrides it.
+int host_chunk(int batch, long floats_per_field) {
+  if (const char *e = getenv("TS_HOST_CHUNK")) {
+    const int c = atoi(e);
+    if (c > 0) return std::min(c, batch);
+  }
+  if (batch < 32) return batch;
+  long c = ((batch + 3) / 4 + 15) / 16 * 16;
+  const long cap = std::max(16L, (64L << 20) / (4 * floats_per_field) / 16 * 16);
+  return (int)std::min<long>(std::min(c, cap), batch);
+}
+
+void ensure_copy_streams(ts_ctx ctx, size_t nevents) {
+  if (!ctx->copy_in) TS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
+  if (!ctx->copy_out) TS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
+  while (ctx->events.size() < nevents) {
+    cudaEvent_t e;
+    TS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->events.push_back(e);
+  }
+}
+
+// A blocking host-array transform as a pipeline over chunks of fields:
+// chunk c's host->device copy (copy_in stream), its transform `fn` (the
+// context's stream) and its device->host copy (copy_out stream) are ordered
+// by events, so copies of one chunk overlap the transform of another and the
+// two copy directions run at once.  `din`/`dout` are device staging arrays
+// for the whole batch (each chunk has its own slice, so nothing is reused
+// while in flight).  All host->device copies and transforms are enqueued
+// before the first device->host copy: a pageable destination makes that copy
+// block the host until its chunk is done, which then delays nothing else.
+// Page-locked host arrays (cudaHostAlloc, cudaHostRegister) give the full
+// overlap; pageable ones are copied through the driver's staging.  Returns
+// when every copy has landed; on an error it waits for whatever was enqueued
+// before rethrowing, so no copy still touches the caller's arrays.
+template <class Fn>
+void host_pipeline(ts_plan p, const float *in, long in_pf, float *din, float *out, long out_pf,
+                   float *dout, int batch, int chunk, Fn fn) {
+  ts_ctx ctx = p->ctx;
+  const int nch = (batch + chunk - 1) / chunk;
+  ensure_copy_streams(ctx, 2 * (size_t)nch + 1);
+  cudaStream_t s = ctx->stream;
+  try {
+    // the staging arrays are idle once the work queued before this call is done
+    TS_CUDA(cudaEventRecord(ctx->events[2 * nch], s));
+    TS_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->events[2 * nch], 0));
+    for (int c = 0; c < nch; c++) {
+      const long f0 = (long)c * chunk;
+      const int nf = std::min<int>(chunk, batch - (int)f0);
+      TS_CUDA(cudaMemcpyAsync(din + f0 * in_pf, in + f0 * in_pf, sizeof(float) * nf * in_pf,
+                              cudaMemcpyHostToDevice, ctx->copy_in));
+      TS_CUDA(cudaEventRecord(ctx->events[2 * c], ctx->copy_in));
+      TS_CUDA(cudaStreamWaitEvent(s, ctx->events[2 * c], 0));
+      fn(din + f0 * in_pf, dout + f0 * out_pf, nf, s);
+      TS_CUDA(cudaEventRecord(ctx->events[2 * c + 1], s));
+    }
+    for (int c = 0; c < nch; c++) {
+      const long f0 = (long)c * chunk;
+      const int nf = std::min<int>(chunk, batch - (int)f0);
+      TS_CUDA(cudaStreamWaitEvent(ctx->copy_out, ctx->events[2 * c + 1], 0));
+      TS_CUDA(cudaMemcpyAsync(out + f0 * out_pf, dout + f0 * out_pf, sizeof(float) * nf * out_pf,
+                              cudaMemcpyDeviceToHost, ctx->copy_out));
+    }
+    TS_CUDA(cudaStreamSynchronize(ctx->copy_out));
+    TS_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    cudaStreamSynchronize(ctx->copy_in);
+    cudaStreamSynchronize(s);
+    cudaStreamSynchronize(ctx->copy_out);
+    throw;
+  }
+}
+}  // namespace
+
+ts_device_guard::ts_device_guard(int device, bool nothrow) {
+  const ts_ctx_fns &f = ctx_fns();
+  CUcontext prev = nullptr;
+  if (f.get && f.get(&prev) == CUDA_SUCCESS) {
+    prev_ = (void *)prev;
+    saved_ = true;
+  }
+  const cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    ok_ = false;
+    if (!nothrow) {
+      saved_ = false;  // the destructor does not run when the constructor throws
+      ts_throw(TS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+  }
+}
+
+ts_device_guard::~ts_device_guard() {
+  if (!saved_) return;
+  const ts_ctx_fns &f = ctx_fns();
+  CUcontext cur = nullptr;
+  if (f.get(&cur) == CUDA_SUCCESS && cur != (CUcontext)prev_) f.set((CUcontext)prev_);
+}
+
 extern "C" {
 
 // ------------------------------------------------------------------ context
@@ -150,7 +299,7 @@ int ts_ctx_create(int device_ordinal, ts_ctx *out) {
                "device ordinal out of range");
     ctx = new ts_ctx_s();
     ctx->device = device_ordinal;
-    TS_CUDA(cudaSetDevice(device_ordinal));
+    ts_device_guard dev_guard_(device_ordinal);
     cudaDeviceProp prop;
     TS_CUDA(cudaGetDeviceProperties(&prop, device_ordinal));
     ctx->sm_count = prop.multiProcessorCount;
@@ -173,11 +322,17 @@ int ts_ctx_create(int device_ordinal, ts_ctx *out) {
 
 int ts_ctx_destroy(ts_ctx ctx) {
   if (!ctx) return TS_ERR_INVALID;
-  cudaSetDevice(ctx->device);
+  ts_device_guard dev_guard_(ctx->device, true);
   if (ctx->own_stream) {
     cudaStreamSynchronize(ctx->own_stream);
     cudaStreamDestroy(ctx->own_stream);
   }
+  for (cudaStream_t st : {ctx->copy_in, ctx->copy_out})
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   delete ctx;
   return TS_OK;
 }
@@ -201,7 +356,7 @@ int ts_ctx_device_name(ts_ctx ctx, char *buf, size_t cap) {
 int ts_sync(ts_ctx ctx) {
   TS_API_BEGIN
   TS_REQUIRE(ctx != nullptr, TS_ERR_INVALID, "null context");
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   TS_CUDA(cudaStreamSynchronize(ctx->stream));
   TS_API_END(ctx)
 }
@@ -241,7 +396,7 @@ int ts_sht_plan_create(ts_ctx ctx, int lmax, int mmax, int nlat, int nphi, int f
     TS_REQUIRE(out != nullptr, TS_ERR_INVALID, "null output handle");
     const std::string e = config_error(lmax, mmax, nlat, nphi);
     TS_REQUIRE(e.empty(), TS_ERR_INVALID, e);
-    TS_CUDA(cudaSetDevice(ctx->device));
+    ts_device_guard dev_guard_(ctx->device);
     p = new ts_plan_s();
     p->ctx = ctx;
     p->lmax = lmax;
@@ -286,7 +441,7 @@ int ts_sht_plan_create(ts_ctx ctx, int lmax, int mmax, int nlat, int nphi, int f
 
 int ts_sht_plan_destroy(ts_plan p) {
   if (!p) return TS_ERR_INVALID;
-  cudaSetDevice(p->ctx->device);
+  ts_device_guard dev_guard_(p->ctx->device, true);
   cudaStreamSynchronize(p->ctx->stream);
   plan_free(p);
   delete p;
@@ -327,7 +482,7 @@ int ts_sht_plan_test_stall(ts_plan p, int stall_copies, unsigned wait_limit) {
   TS_API_BEGIN
   TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
   TS_REQUIRE(p->tc != nullptr, TS_ERR_UNSUPPORTED, "FP32 plans have no bounded waits");
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   TS_CUDA(cudaStreamSynchronize(ctx->stream));
   ts_tc_set_fault(p, stall_copies, wait_limit);
   TS_API_END(ctx)
@@ -337,7 +492,7 @@ int ts_sht_plan_status(ts_plan p) {
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
   TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   TS_CUDA(cudaStreamSynchronize(ctx->stream));
   if (ts_tc_check_error(p)) {
     int zero = 0;
@@ -360,7 +515,7 @@ int ts_sht_synth_dev(ts_plan p, const float *qlm, float *spat, int batch, void *
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
   check_batch(p, qlm, spat, batch);
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   synth_dev(p, qlm, spat, batch, ts_pick_stream(ctx, stream));
   TS_API_END(ctx)
 }
@@ -369,7 +524,7 @@ int ts_sht_analys_dev(ts_plan p, const float *spat, float *qlm, int batch, void 
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
   check_batch(p, spat, qlm, batch);
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   analys_dev(p, spat, qlm, batch, ts_pick_stream(ctx, stream));
   TS_API_END(ctx)
 }
@@ -378,20 +533,18 @@ int ts_sht_synth(ts_plan p, const float *qlm, long qlm_len, float *spat, long sp
                  int batch) {
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
-  check_batch(p, qlm, spat, batch);
-  char buf[128];
-  snprintf(buf, sizeof buf, "qlm must have length %ld", 2 * p->nlm * batch);
-  TS_REQUIRE(qlm_len == 2 * p->nlm * batch, TS_ERR_SIZE, buf);
-  snprintf(buf, sizeof buf, "spat must have length %ld", npts_of(p) * batch);
-  TS_REQUIRE(spat_len == npts_of(p) * batch, TS_ERR_SIZE, buf);
-  TS_CUDA(cudaSetDevice(ctx->device));
-  cudaStream_t s = ctx->stream;
-  p->stage_q.ensure(sizeof(float) * qlm_len);
-  p->stage_s.ensure(sizeof(float) * spat_len);
-  TS_CUDA(cudaMemcpyAsync(p->stage_q.p, qlm, sizeof(float) * qlm_len, cudaMemcpyHostToDevice, s));
-  synth_dev(p, (const float *)p->stage_q.p, (float *)p->stage_s.p, batch, s);
-  TS_CUDA(cudaMemcpyAsync(spat, p->stage_s.p, sizeof(float) * spat_len, cudaMemcpyDeviceToHost, s));
-  TS_CUDA(cudaStreamSynchronize(s));
+  check_host_batch(p, qlm, spat, batch);
+  require_len("qlm", qlm_len, 2 * p->nlm * batch);
+  require_len("spat", spat_len, npts_of(p) * batch);
+  ts_device_guard dev_guard_(ctx->device);
+  const int chunk = host_chunk(batch, std::max<long>(2 * p->nlm, npts_of(p)));
+  p->stage_q.ensure(sizeof(float) * 2 * p->nlm * batch);
+  p->stage_s.ensure(sizeof(float) * npts_of(p) * batch);
+  host_pipeline(p, qlm, 2 * p->nlm, (float *)p->stage_q.p, spat, npts_of(p),
+                (float *)p->stage_s.p, batch, chunk,
+                [&](const float *din, float *dout, int nf, cudaStream_t s) {
+                  synth_dev(p, din, dout, nf, s);
+                });
   TS_API_END(ctx)
 }
 
@@ -399,20 +552,40 @@ int ts_sht_analys(ts_plan p, const float *spat, long spat_len, float *qlm, long 
                   int batch) {
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
-  check_batch(p, spat, qlm, batch);
-  char buf[128];
-  snprintf(buf, sizeof buf, "spat must have length %ld", npts_of(p) * batch);
-  TS_REQUIRE(spat_len == npts_of(p) * batch, TS_ERR_SIZE, buf);
-  snprintf(buf, sizeof buf, "qlm must have length %ld", 2 * p->nlm * batch);
-  TS_REQUIRE(qlm_len == 2 * p->nlm * batch, TS_ERR_SIZE, buf);
-  TS_CUDA(cudaSetDevice(ctx->device));
-  cudaStream_t s = ctx->stream;
-  p->stage_q.ensure(sizeof(float) * qlm_len);
-  p->stage_s.ensure(sizeof(float) * spat_len);
-  TS_CUDA(cudaMemcpyAsync(p->stage_s.p, spat, sizeof(float) * spat_len, cudaMemcpyHostToDevice, s));
-  analys_dev(p, (const float *)p->stage_s.p, (float *)p->stage_q.p, batch, s);
-  TS_CUDA(cudaMemcpyAsync(qlm, p->stage_q.p, sizeof(float) * qlm_len, cudaMemcpyDeviceToHost, s));
-  TS_CUDA(cudaStreamSynchronize(s));
+  check_host_batch(p, spat, qlm, batch);
+  require_len("spat", spat_len, npts_of(p) * batch);
+  require_len("qlm", qlm_len, 2 * p->nlm * batch);
+  ts_device_guard dev_guard_(ctx->device);
+  const int chunk = host_chunk(batch, std::max<long>(2 * p->nlm, npts_of(p)));
+  p->stage_s.ensure(sizeof(float) * npts_of(p) * batch);
+  p->stage_q.ensure(sizeof(float) * 2 * p->nlm * batch);
+  host_pipeline(p, spat, npts_of(p), (float *)p->stage_s.p, qlm, 2 * p->nlm,
+                (float *)p->stage_q.p, batch, chunk,
+                [&](const float *din, float *dout, int nf, cudaStream_t s) {
+                  analys_dev(p, din, dout, nf, s);
+                });
+  TS_API_END(ctx)
+}
+
+int ts_sht_roundtrip(ts_plan p, const float *qlm_in, long in_len, float *qlm_out, long out_len,
+                     int batch) {
+  ts_ctx ctx = p ? p->ctx : nullptr;
+  TS_API_BEGIN
+  check_host_batch(p, qlm_in, qlm_out, batch);
+  require_len("qlm_in", in_len, 2 * p->nlm * batch);
+  require_len("qlm_out", out_len, 2 * p->nlm * batch);
+  ts_device_guard dev_guard_(ctx->device);
+  const int chunk = host_chunk(batch, 2 * p->nlm);
+  p->stage_q.ensure(sizeof(float) * 2 * p->nlm * batch);
+  p->stage_q2.ensure(sizeof(float) * 2 * p->nlm * batch);
+  p->stage_s.ensure(sizeof(float) * npts_of(p) * chunk);
+  float *grid = (float *)p->stage_s.p;
+  host_pipeline(p, qlm_in, 2 * p->nlm, (float *)p->stage_q.p, qlm_out, 2 * p->nlm,
+                (float *)p->stage_q2.p, batch, chunk,
+                [&](const float *din, float *dout, int nf, cudaStream_t s) {
+                  synth_dev(p, din, grid, nf, s);
+                  analys_dev(p, grid, dout, nf, s);
+                });
   TS_API_END(ctx)
 }
 
@@ -420,7 +593,7 @@ int ts_sht_leg_synth_dev(ts_plan p, const float *qlm, float *fm, int batch, void
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
   check_batch(p, qlm, fm, batch);
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   ts_launch_leg_synth(p, (const float2 *)qlm, p->nlm, (float2 *)fm, (long)(p->mmax + 1) * p->nlat,
                       batch, ts_pick_stream(ctx, stream));
   TS_API_END(ctx)
@@ -430,7 +603,7 @@ int ts_sht_fourier_synth_dev(ts_plan p, const float *fm, float *spat, int batch,
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
   check_batch(p, fm, spat, batch);
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   ts_launch_fourier_synth(p, (const float2 *)fm, (long)(p->mmax + 1) * p->nlat, spat, npts_of(p),
                           batch, ts_pick_stream(ctx, stream));
   TS_API_END(ctx)
@@ -440,7 +613,7 @@ int ts_sht_fourier_analys_dev(ts_plan p, const float *spat, float *fm, int batch
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
   check_batch(p, spat, fm, batch);
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   ts_launch_fourier_analys(p, spat, npts_of(p), (float2 *)fm, (long)(p->mmax + 1) * p->nlat,
                            batch, ts_pick_stream(ctx, stream));
   TS_API_END(ctx)
@@ -450,7 +623,7 @@ int ts_sht_leg_analys_dev(ts_plan p, const float *fm, float *qlm, int batch, voi
   ts_ctx ctx = p ? p->ctx : nullptr;
   TS_API_BEGIN
   check_batch(p, fm, qlm, batch);
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   ts_launch_leg_analys(p, (const float2 *)fm, (long)(p->mmax + 1) * p->nlat, (float2 *)qlm,
                        p->nlm, batch, ts_pick_stream(ctx, stream));
   TS_API_END(ctx)
@@ -467,7 +640,7 @@ int ts_sht_fourier_analys_w_dev(ts_plan p, const float *spat, void *wimage, int 
   TS_API_BEGIN
   check_batch(p, spat, wimage, batch);
   TS_REQUIRE(p->precision != TS_PREC_FP32, TS_ERR_UNSUPPORTED, "FP32 plans have no W image");
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   TS_REQUIRE(ts_launch_fourier_analys_w(p, spat, npts_of(p), batch, TS_TC_FIELDS, (char *)wimage,
                                         ts_pick_stream(ctx, stream)),
              TS_ERR_UNSUPPORTED, "the plan's row length has no two-phase FFT shape");
@@ -479,7 +652,7 @@ int ts_sht_leg_analys_w_dev(ts_plan p, const void *wimage, float *qlm, int batch
   TS_API_BEGIN
   check_batch(p, wimage, qlm, batch);
   TS_REQUIRE(p->precision != TS_PREC_FP32, TS_ERR_UNSUPPORTED, "FP32 plans have no W image");
-  TS_CUDA(cudaSetDevice(ctx->device));
+  ts_device_guard dev_guard_(ctx->device);
   ts_launch_analys_tc_img(p, (const char *)wimage, batch, (float2 *)qlm, p->nlm,
                           ts_pick_stream(ctx, stream));
   TS_API_END(ctx)

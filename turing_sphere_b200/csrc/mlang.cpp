@@ -421,7 +421,7 @@ double fold_call(const std::string &fn, double a, double b) {
   if (fn == "log2") return std::log2(a);
   if (fn == "max") return std::fmax(a, b);
   if (fn == "min") return std::fmin(a, b);
-  if (fn == "round") return std::round(a);
+  if (fn == "round") return std::nearbyint(a);  // ties to even, as WGSL round (wgsl.ts:64)
   if (fn == "sign") return (a > 0) - (a < 0);
   if (fn == "sin") return std::sin(a);
   if (fn == "sinh") return std::sinh(a);

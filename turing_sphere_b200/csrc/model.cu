@@ -101,7 +101,7 @@ const std::map<std::string, std::string> kCudaFn = {
     {"abs", "fabsf"},   {"acos", "acosf"},   {"asin", "asinf"}, {"atan", "atanf"},
     {"atan2", "atan2f"}, {"ceil", "ceilf"},  {"cos", "cosf"},   {"cosh", "coshf"},
     {"exp", "expf"},    {"floor", "floorf"}, {"log", "logf"},   {"log2", "log2f"},
-    {"max", "fmaxf"},   {"min", "fminf"},    {"round", "roundf"}, {"sign", "ts_sign"},
+    {"max", "fmaxf"},   {"min", "fminf"},    {"round", "rintf"}, {"sign", "ts_sign"},
     {"sin", "sinf"},    {"sinh", "sinhf"},   {"sqrt", "sqrtf"}, {"tan", "tanf"},
     {"tanh", "tanhf"}, {"__ge_sel", "ts_ge_sel"}};
 
@@ -1367,7 +1367,7 @@ int ts_model_compile(ts_plan plan, const char *source, const char *const *state,
     TS_REQUIRE(batch >= 1 && batch <= 65535, TS_ERR_INVALID, "batch must be in [1, 65535]");
     TS_REQUIRE(plan->fourier == TS_FOURIER_FFT, TS_ERR_UNSUPPORTED,
                "models need an FFT grid: nphi = 2^a 3^b (the fused phase kernel runs the FFT)");
-    TS_CUDA(cudaSetDevice(ctx->device));
+    ts_device_guard dev_guard_(ctx->device);
     m = new ts_model_s();
     m->ctx = ctx;
     m->plan = plan;
@@ -1426,7 +1426,7 @@ int ts_model_compile(ts_plan plan, const char *source, const char *const *state,
 
 int ts_model_destroy(ts_model m) {
   if (!m) return TS_ERR_INVALID;
-  cudaSetDevice(m->ctx->device);
+  ts_device_guard dev_guard_(m->ctx->device, true);
   cudaStreamSynchronize(m->ctx->stream);
   free_model(m);
   delete m;
@@ -1437,7 +1437,7 @@ int ts_model_destroy(ts_model m) {
   ts_ctx ctx = m ? m->ctx : nullptr;                   \
   try {                                                \
     TS_REQUIRE(m != nullptr, TS_ERR_INVALID, "null model"); \
-    TS_CUDA(cudaSetDevice(ctx->device));
+    ts_device_guard dev_guard_(ctx->device);
 #define TSM_END                                         \
   }                                                     \
   catch (const ts_exc &e) {                             \
@@ -1624,7 +1624,7 @@ int ts_model_group_create(ts_model const *models, int n, ts_group *out) {
     for (int i = 0; i < n; i++)
       TS_REQUIRE(models[i] && models[i]->ctx == ctx, TS_ERR_INVALID,
                  "group: every model must belong to the same context");
-    TS_CUDA(cudaSetDevice(ctx->device));
+    ts_device_guard dev_guard_(ctx->device);
     g = new ts_group_s();
     g->models.assign(models, models + n);
     TS_CUDA(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
@@ -1649,7 +1649,7 @@ int ts_model_group_step(ts_group g, int nsteps) {
   ts_ctx ctx = g && !g->models.empty() ? g->models[0]->ctx : nullptr;
   try {
     TS_REQUIRE(g != nullptr && nsteps >= 0, TS_ERR_INVALID, "bad group or step count");
-    TS_CUDA(cudaSetDevice(ctx->device));
+    ts_device_guard dev_guard_(ctx->device);
     const cudaStream_t s0 = ctx->stream;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     const bool capturable = g->use_graphs && s0 != nullptr && s0 != cudaStreamLegacy &&
@@ -1677,10 +1677,8 @@ int ts_model_group_step(ts_group g, int nsteps) {
 
 int ts_model_group_destroy(ts_group g) {
   if (!g) return TS_ERR_INVALID;
-  if (!g->models.empty()) {
-    cudaSetDevice(g->models[0]->ctx->device);
-    cudaStreamSynchronize(g->models[0]->ctx->stream);
-  }
+  ts_device_guard dev_guard_(g->models.empty() ? 0 : g->models[0]->ctx->device, true);
+  if (!g->models.empty()) cudaStreamSynchronize(g->models[0]->ctx->stream);
   for (auto &x : g->graphs) cudaGraphExecDestroy(x.exec);
   for (cudaStream_t st : g->streams) cudaStreamDestroy(st);
   for (cudaEvent_t ev : g->done) cudaEventDestroy(ev);

@@ -54,6 +54,7 @@ extern "C" int ts_sht_synth_noalloc(ts_plan p, const float *qlm, float *spat, in
     TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
     TS_REQUIRE(qlm != nullptr && spat != nullptr, TS_ERR_INVALID, "null buffer");
     TS_REQUIRE(batch >= 1 && batch <= 65535, TS_ERR_INVALID, "batch must be in [1, 65535]");
+    ts_require_aligned8(qlm, spat);
     const long fm_stride = (long)(p->mmax + 1) * p->nlat;
     const size_t need = sizeof(float2) * (size_t)fm_stride * (size_t)batch;
     if (need > TS_NOALLOC_SCRATCH_BYTES) {
@@ -65,7 +66,7 @@ extern "C" int ts_sht_synth_noalloc(ts_plan p, const float *qlm, float *spat, in
                (long)(TS_NOALLOC_SCRATCH_BYTES / (sizeof(float2) * (size_t)fm_stride)));
       ts_throw(TS_ERR_SIZE, buf);
     }
-    TS_CUDA(cudaSetDevice(ctx->device));
+    ts_device_guard dev_guard_(ctx->device);
     float2 *fm = noalloc_scratch(ctx->device);
     // The Legendre stage writes every (field, m, latitude) entry the Fourier
     // stage then reads, so nothing left in the array by an earlier call is used.

@@ -1,6 +1,7 @@
 // Internal runtime types of libturing_sht.so (not part of the C ABI).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -30,12 +31,48 @@ struct ts_exc {
     if (!(cond)) ts_throw(code, msg); \
   } while (0)
 
+// Device arrays of the transforms hold complex pairs and grid rows that the
+// kernels read and write as float2 (8 bytes); a float pointer that is only
+// 4-byte aligned is refused before any launch.
+inline void ts_require_aligned8(const void *a, const void *b) {
+  TS_REQUIRE(((reinterpret_cast<unsigned long long>(a) | reinterpret_cast<unsigned long long>(b)) &
+              7) == 0,
+             TS_ERR_INVALID,
+             "device arrays must be 8-byte aligned (coefficient pairs and grid rows are read "
+             "as float2)");
+}
+
+// Makes `device` current for the lifetime of the guard (one C-ABI call) and
+// then gives the calling thread back the CUDA context it had before the call,
+// including none: a caller working on another device, or one that never
+// touched CUDA, finds its thread as it left it.  The saved context is read
+// and restored through the driver (cuCtxGetCurrent / cuCtxSetCurrent, looked
+// up once through the runtime), so restoring never creates a primary context
+// on a device the caller did not use.  `nothrow` guards (destroy calls) report
+// a failed cudaSetDevice by leaving ok() false instead of throwing.
+class ts_device_guard {
+ public:
+  explicit ts_device_guard(int device, bool nothrow = false);
+  ~ts_device_guard();
+  bool ok() const { return ok_; }
+  ts_device_guard(const ts_device_guard &) = delete;
+  ts_device_guard &operator=(const ts_device_guard &) = delete;
+
+ private:
+  void *prev_ = nullptr;  // CUcontext current on entry (may be null)
+  bool saved_ = false, ok_ = true;
+};
+
 struct ts_ctx_s {
   int device = 0;
   int sm_count = 0;
   size_t smem_optin = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  // host-array transforms: copy streams (host->device, device->host) and a
+  // pool of ordering events, created on first use
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  std::vector<cudaEvent_t> events;
   std::string err;
   std::string name;
 };
@@ -74,7 +111,7 @@ struct ts_plan_s {
   TsLegTab leg{};
   TsFftTab fft{};
   // scratch: fm intermediate, host-call staging, adjoint scalings
-  ts_dbuf fm, stage_q, stage_s, adj_grid, adj_spec;
+  ts_dbuf fm, stage_q, stage_s, stage_q2, adj_grid, adj_spec;
   // tensor-core tables (precision != FP32)
   void *tc = nullptr;
   // kernel shapes: 0 = default (or TS_TC_NL / TS_TC_LTL); set by the autotuner

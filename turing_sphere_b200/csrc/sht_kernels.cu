@@ -292,16 +292,17 @@ int pick_lb(ts_plan p, int nfields, int nbuf, size_t *smem_out) {
 }  // namespace
 
 void ts_kernel_attrs_once(ts_ctx ctx) {
-  static bool done = false;  // attributes are per-function, not per-device
-  if (done) return;
-  const int cap = (int)ctx->smem_optin;
-  TS_CUDA(cudaFuncSetAttribute(ts_leg_synth_f32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-  TS_CUDA(cudaFuncSetAttribute(ts_leg_synth_f32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-  TS_CUDA(cudaFuncSetAttribute(ts_leg_synth_f32<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-  TS_CUDA(cudaFuncSetAttribute(ts_leg_synth_f32<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-  TS_CUDA(cudaFuncSetAttribute(ts_fourier_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-  TS_CUDA(cudaFuncSetAttribute(ts_fourier_analys, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
-  done = true;
+  // cudaFuncSetAttribute acts on the current device's copy of a kernel, so
+  // the limits are raised per (device, kernel): a context on a second GPU of
+  // the process gets its own (ts_allow_smem keys its record by device).
+  const size_t cap = ctx->smem_optin;
+  const int dev = ctx->device;
+  ts_allow_smem((const void *)ts_leg_synth_f32<1>, dev, cap);
+  ts_allow_smem((const void *)ts_leg_synth_f32<2>, dev, cap);
+  ts_allow_smem((const void *)ts_leg_synth_f32<4>, dev, cap);
+  ts_allow_smem((const void *)ts_leg_synth_f32<8>, dev, cap);
+  ts_allow_smem((const void *)ts_fourier_synth, dev, cap);
+  ts_allow_smem((const void *)ts_fourier_analys, dev, cap);
 }
 
 void ts_launch_leg_synth_fields(ts_plan p, const TsFields &q, float2 *fm, long fs, int nf,

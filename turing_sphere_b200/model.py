@@ -303,16 +303,10 @@ class ModelSession:
         synthesised on the oversampled grid (session.ts:201-207)."""
         if not self._displaySht:
             return self.read(self.model.species[k])
-        ptr, _ = self.gpu.valueBuffer(self.model.state[k])
-        d = self._displaySht
-        out = np.empty(d.cfg.nlat * d.cfg.nphi, dtype=np.float32)
-        import torch  # device scratch for the display grid
-        spat = torch.empty(out.size, dtype=torch.float32, device=f"cuda:{self.device.ordinal}")
-        self.device.sync()
-        d.synth_dev(ptr, spat.data_ptr(), 1, None)
-        self.device.sync()
-        out[:] = spat.cpu().numpy()
-        return out
+        # the spectral state (2 nlm floats) comes back to the host and the
+        # display plan synthesises it through its own staging buffers
+        q = self.gpu.read(self.model.state[k], 0)
+        return self._displaySht.synth(q)
 
     def describe(self) -> dict:
         return self.gpu.describe()

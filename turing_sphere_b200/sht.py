@@ -137,6 +137,25 @@ class ShtPlan:
                                             out.size, batch), self.device.handle)
         return out
 
+    def roundtrip(self, qlm, batch: int = 1, out=None) -> np.ndarray:
+        """analys(synth(qlm)) per field with host arrays in and out and the
+        grid kept on the device: the round trip of scripts/bench-sht.ts:190-217
+        as one blocking call (ts_sht_roundtrip, pipelined over chunks of
+        fields).  `out` may be a preallocated float32 array (e.g. page-locked)."""
+        q = np.ascontiguousarray(qlm, dtype=np.float32).ravel()
+        if q.size != 2 * self.nlm * batch:
+            raise ValueError(f"qlm_in must have length {2 * self.nlm * batch}")
+        if out is None:
+            out = np.empty(q.size, dtype=np.float32)
+        self.roundtrip_ptr(q.ctypes.data, out.ctypes.data, batch)
+        return out
+
+    def roundtrip_ptr(self, in_ptr: int, out_ptr: int, batch: int = 1) -> None:
+        """ts_sht_roundtrip on raw host pointers (2 nlm floats per field each)."""
+        n = 2 * self.nlm * batch
+        _lib.check(_lib.lib().ts_sht_roundtrip(self.handle, in_ptr, n, out_ptr, n, batch),
+                   self.device.handle)
+
     # ---- device-pointer transforms (encodeSynthInto / encodeAnalysInto)
     def synth_dev(self, qlm_ptr: int, spat_ptr: int, batch: int = 1, stream: int | None = None):
         _lib.check(_lib.lib().ts_sht_synth_dev(self.handle, qlm_ptr, spat_ptr, batch, stream),
