@@ -239,8 +239,12 @@ def cpu_baselines_extra():
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU transform path, restated (oracle)."""
+    """--impl reference: the reference's CPU transform path (src/sht/reference.ts,
+    restated in C by the oracle: the reference itself is TypeScript on WebGPU
+    and cannot run here) on all host cores, rank 0 only, on a bounded sample
+    of this arm's workload: `per_step` single-field pairs per step."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     from oracle import oracle as O
@@ -263,11 +267,11 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"SHT round trip, lmax {lmax}, {nlat}x{nphi} Gauss grid, "
-                               f"{per_step} fields/step sample of the B={args.batch} batch"},
+        "config": workload_config(lmax, nlat, nphi, args.batch, world),
         "cpu_baseline": {"value": value, "unit": "SHT pairs/s", "cores": cores, "kind": "port",
-                         "sample": f"{per_step} single-field pairs per step, f64 oracle "
-                                   "(src/sht/reference.ts restated in C, OpenMP)"},
+                         "sample": f"{per_step} single-field pairs per step of the B={args.batch} "
+                                   "batch, f64 oracle (src/sht/reference.ts restated in C, "
+                                   "OpenMP over all host cores)"},
         "e2e": {"value": value, "unit": "SHT pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -384,66 +388,73 @@ def time_imex(dev, plan, ninst, K, W, stream):
     return ms, launches, ok
 
 
-def time_e2e(plan, q0, qa, qb, spat, B, K, stream, world, dist):
-    """End to end through the C ABI: every step copies its coefficients from
-    pinned host memory, runs synth + analys and copies the result back.  The
-    copies run on two copy streams (host->device and device->host, full duplex
-    on PCIe) against double-buffered device arrays, so step i's transforms
-    overlap step i+1's upload and step i-1's download, as a serving loop would
-    run them.  Returns (ms for the timed steps, steps, relL2 of the last result)."""
+def time_e2e(plan, q0, B, K, world, dist):
+    """End to end through the library's host-array round trip
+    (ts_sht_roundtrip, the blocking call a reference-shaped host makes: host
+    coefficients in, host coefficients out, the grid kept on the device): every
+    step copies the batch's coefficients from page-locked host memory, runs
+    synth + analys and copies the result back, the library pipelining the
+    copies against the transforms over chunks of fields.  Host wall clock
+    around the blocking calls, max over ranks.  Returns (ms for the timed
+    steps, steps, relL2 of the last result)."""
     import torch
-    hq_in = torch.from_numpy(q0).pin_memory()
-    hq_out = [torch.empty_like(hq_in).pin_memory() for _ in range(2)]
-    d_in = [qa, torch.empty_like(qa)]
-    d_out = [qb, torch.empty_like(qb)]
-    h2d, d2h = torch.cuda.Stream(), torch.cuda.Stream()
-    sp = stream.cuda_stream
+    hin = torch.from_numpy(np.ascontiguousarray(q0).ravel()).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
     Ke = max(3, K // 4)
-    loaded = [torch.cuda.Event() for _ in range(2)]
-    computed = [torch.cuda.Event() for _ in range(2)]
-    saved = [torch.cuda.Event() for _ in range(2)]
-
-    def run(n):
-        for i in range(n):
-            j = i & 1
-            if i >= 2:
-                h2d.wait_event(computed[j])        # step i-2 is done reading d_in[j]
-            with torch.cuda.stream(h2d):
-                d_in[j].copy_(hq_in, non_blocking=True)
-                loaded[j].record(h2d)
-            stream.wait_event(loaded[j])
-            if i >= 2:
-                stream.wait_event(saved[j])        # step i-2's result has left d_out[j]
-            plan.synth_dev(d_in[j].data_ptr(), spat.data_ptr(), B, sp)
-            plan.analys_dev(spat.data_ptr(), d_out[j].data_ptr(), B, sp)
-            computed[j].record(stream)
-            d2h.wait_event(computed[j])
-            with torch.cuda.stream(d2h):
-                hq_out[j].copy_(d_out[j], non_blocking=True)
-                saved[j].record(d2h)
-        stream.wait_stream(h2d)
-        stream.wait_stream(d2h)
-
-    run(3)
+    for _ in range(2):  # grows the plan's staging arrays
+        plan.roundtrip_ptr(hin.data_ptr(), hout.data_ptr(), B)
     if world > 1:
         dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    h2d.wait_event(e0)
-    d2h.wait_event(e0)
-    run(Ke)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ems = e0.elapsed_time(e1)
+    t0 = time.perf_counter()
+    for _ in range(Ke):
+        plan.roundtrip_ptr(hin.data_ptr(), hout.data_ptr(), B)
+    ems = (time.perf_counter() - t0) * 1e3
     if world > 1:
         t = torch.tensor([ems], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ems = float(t.item())
-    back = hq_out[(Ke - 1) & 1].numpy()
-    err = float(np.sqrt(((back - q0) ** 2).sum() / (q0 ** 2).sum()))
+    back = hout.numpy()
+    ref = hin.numpy()
+    err = float(np.sqrt(((back - ref) ** 2).sum() / (ref ** 2).sum()))
     return ems, Ke, err
+
+
+def time_host_grid_pairs(plan, q0, B, K=3):
+    """SHT pairs through the two host-array calls of the reference's ShtPlan
+    (synth(Float32Array) -> grid on the host -> analys(Float32Array),
+    sht.ts:414-461): the grid crosses PCIe both ways, 4.5x the bytes of the
+    round trip.  Page-locked host arrays; host wall clock.  Returns pairs/s."""
+    import torch
+    nq, ns = q0.size, B * plan.cfg.nlat * plan.cfg.nphi
+    hq = torch.from_numpy(np.ascontiguousarray(q0).ravel()).pin_memory()
+    hs = torch.empty(ns, dtype=torch.float32).pin_memory()
+    ho = torch.empty(nq, dtype=torch.float32).pin_memory()
+    L, h = plan_lib(), plan.handle
+
+    def step():
+        chk(L.ts_sht_synth(h, ptr(hq), nq, ptr(hs), ns, B), plan)
+        chk(L.ts_sht_analys(h, ptr(hs), ns, ptr(ho), nq, B), plan)
+
+    step()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        step()
+    return B * K / (time.perf_counter() - t0)
+
+
+def plan_lib():
+    from turing_sphere_b200 import _lib
+    return _lib.lib()
+
+
+def ptr(t):
+    import ctypes as C
+    return C.cast(t.data_ptr(), C.POINTER(C.c_float))
+
+
+def chk(rc, plan):
+    from turing_sphere_b200 import _lib
+    _lib.check(rc, plan.device.handle)
 
 
 def time_imex_single_lmax63(dev, stream, precision, K=2000, graphs=True):
@@ -479,17 +490,11 @@ def time_brusselator_sweep(dev, stream, K=200):
     Turing-unstable band, lmax 127 on 192 x 384, tensor-core plan, steps as
     captured graphs.  Returns instance-steps/s."""
     import torch
-    from turing_sphere_b200 import (GpuModel, ShtConfig, ShtPlan, defaultParams, mModelByKey,
-                                    seededNoise)
+    from turing_sphere_b200 import GpuModel, ShtConfig, ShtPlan, mModelByKey, seededNoise
+    from turing_sphere_b200.registry import brusselatorSweep
     model = mModelByKey("brusselator")
-    base = defaultParams(model)
     ni, npts = 256, 192 * 384
-    rng = np.random.default_rng(3)
-    sweep = []
-    for _ in range(ni):
-        a = rng.uniform(2.5, 3.5)
-        lo = (1 + a * math.sqrt(base["D1"] / base["D2"])) ** 2
-        sweep.append(dict(base, A=a, B=rng.uniform(lo, 1 + a * a)))
+    sweep = brusselatorSweep(ni, seed=3)
     plan = ShtPlan.create(dev, ShtConfig(127, 127, 192, 384), {"precision": "tf32x3",
                                                                "autotune": True})
     gpu = GpuModel.create(dev, plan, model.source, [q.key for q in model.params], model.state,
@@ -577,8 +582,26 @@ def time_adjoint(dev, key, lmax, nlat, nphi, ni, nsteps, every):
     return dt, ok
 
 
+def launch_ranks(n):
+    """`bench.py --gpus N` run without a launcher: start N ranks (one per GPU)
+    under torch.distributed.run on 127.0.0.1 with the same arguments, and
+    return their exit status.  Under a launcher (WORLD_SIZE set) it is not
+    called."""
+    import socket
+    import subprocess
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -672,20 +695,24 @@ def main():
                   flush=True)
         return finish(plan, plain, dev, world)
 
-    ems, Ke, e2e_err = time_e2e(plan, q0, qa, qb, spat, B, K, stream, world, dist)
+    # free the transform buffers before the model workloads
+    del spat, fm, qa, qb
+    torch.cuda.empty_cache()
+    ems, Ke, e2e_err = time_e2e(plan, q0, B, K, world, dist)
+    host_grid = time_host_grid_pairs(plan, q0, B)
 
     # IMEX steps: batched Schnakenberg instances on the same grid, both precisions
-    del spat, fm
-    torch.cuda.empty_cache()
     ni = args.imex_instances
     imex_tc_ms, imex_launches, ok_tc = time_imex(dev, plan, ni, args.imex_steps, 3, stream)
-    imex_fp_ms, _, ok_fp = time_imex(dev, plain, ni, max(10, args.imex_steps // 4), 3, stream)
+    kfp = max(10, args.imex_steps // 4)
+    imex_fp_ms, _, ok_fp = time_imex(dev, plain, ni, kfp, 3, stream)
     c1_fp32 = time_imex_single_lmax63(dev, stream, "fp32")
     c1_tc = time_imex_single_lmax63(dev, stream, "tf32x3")
-    c3 = time_brusselator_sweep(dev, stream)
-    c3["ragged"] = time_ragged(dev, stream)
-    a4_s, a4_ok = time_adjoint(dev, "allencahn", 255, 384, 768, 1, 256, 32)
-    a5_s, a5_ok = time_adjoint(dev, "schnakenberg", 511, 768, 1536, 64, 64, 32)
+    c3 = time_brusselator_sweep(dev, stream, K=5000)
+    c3["ragged"] = time_ragged(dev, stream, K=5000)
+    a4_s, a4_ok = time_adjoint(dev, "allencahn", 255, 384, 768, 1, 1000, 32)
+    a5_s, a5_ok = time_adjoint(dev, "schnakenberg", 511, 768, 1536, 64, 500, 32)
+    c5 = time_forward_lmax511(dev, stream)
 
     if rank == 0:
         hbm, bf16, src = measured_peaks()
@@ -704,11 +731,15 @@ def main():
         passes = 3 if args.precision != "fp32" else 1
         of = "of measured" if src == "measured" else "of fallback"
 
-        roof = stage_roofline(name, stage_ms[name], alg_bytes[name], leg_flop, passes, hbm, bf16,
-                              of)
-        roof["traffic"] = profiled_traffic(name)
-        roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                  "launch (profiles/sht_pair_lmax255_b256_kernels.txt)")
+        roof = pair_roofline(ms / K, B, bytes_per_pair(lmax, lmax, nlat, nphi), hbm, of)
+        roof["traffic"] = profiled_pair_traffic(stages)
+        roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, summed over "
+                                  "the pair's kernels, one launch each "
+                                  "(profiles/sht_pair_lmax255_b256_kernels.txt)")
+        dom = stage_roofline(name, stage_ms[name], alg_bytes[name], leg_flop, passes, hbm, bf16,
+                             of)
+        dom["traffic"] = profiled_traffic(name)
+        roof["dominant_kernel"] = dom
         roof["stage_ms"] = stage_ms
         roof["stages"] = {
             st: {k: v for k, v in stage_roofline(st, stage_ms[st], alg_bytes[st], leg_flop, passes,
@@ -718,54 +749,149 @@ def main():
         one = cpu_baseline(lmax, nlat, nphi, budget_s=5.0, threads=1)
         cpu["single_thread"] = {k: one[k] for k in ("value", "cores", "sample")}
         cpu["other_configs"] = cpu_baselines_extra()
+        tc_imex = world * ni * args.imex_steps / (imex_tc_ms / 1e3)
+        fp_imex = world * ni * kfp / (imex_fp_ms / 1e3)
+        plain_pairs = world * B * max(20, K // 4) / (plain_ms / 1e3)
         line = {
             "metric": METRIC, "value": value, "unit": "SHT pairs/s", "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"batched SHT round trip (synth+analys), lmax=mmax={lmax}, "
-                                   f"{nlat}x{nphi} Gauss grid, B={B} fields per GPU",
-                       "precision": args.precision, "fourier": plan.fourierMode,
-                       "fft_radices": plan.fftRadices, "kernel_shapes": plan.shapes,
-                       "global_batch": B * world,
-                       "l2": f"inputs larger than L2 (grid fields {sp_b / 1e6:.0f} MB/step)"},
+            "config": workload_config(lmax, nlat, nphi, B, world),
+            "plan": {"precision": args.precision, "fourier": plan.fourierMode,
+                     "fft_radices": plan.fftRadices, "kernel_shapes": plan.shapes},
             "e2e": {"value": world * B * Ke / (ems / 1e3), "unit": "SHT pairs/s",
                     "h2d_bytes_per_step": int(nlm_b), "d2h_bytes_per_step": int(nlm_b),
-                    "round_trip_rel_l2": e2e_err},
+                    "path": "ts_sht_roundtrip (host coefficients in and out, page-locked; "
+                            "copies pipelined by the library over chunks of fields; host wall "
+                            "clock around the blocking calls)",
+                    "round_trip_rel_l2": e2e_err,
+                    "host_grid_pairs_per_s": host_grid,
+                    "host_grid_path": "ts_sht_synth + ts_sht_analys with the grid on the host "
+                                      "(sht.ts:414-461 shape: 4.5x the PCIe bytes)"},
             "gpu_launches": launches_per_pair(plan) * K,
-            "plain_fp32": {"value": world * B * max(20, K // 4) / (plain_ms / 1e3),
-                           "unit": "SHT pairs/s", "stage_ms": plain_stage},
-            "imex": {"model": "schnakenberg (2 species), D1 sweep", "instances": ni,
-                     "grid": f"lmax {lmax}, {nlat}x{nphi}", "launches_per_step": imex_launches,
-                     "tc_steps_per_s": world * ni * args.imex_steps / (imex_tc_ms / 1e3),
-                     "tc_steps_per_s_per_instance": args.imex_steps / (imex_tc_ms / 1e3),
-                     "fp32_steps_per_s": world * ni * max(10, args.imex_steps // 4) / (imex_fp_ms / 1e3),
-                     "unit": "instance-steps/s", "finite": ok_tc and ok_fp,
-                     "single_lmax63": {"workload": "1 Schnakenberg instance, lmax 63, 96x192, "
-                                             "2000 steps as captured step graphs",
-                                 "fp32_steps_per_s": c1_fp32, "tc_steps_per_s": c1_tc}},
-            "brusselator_sweep_lmax127": c3,
-            "adjoint": {
-                "allencahn_lmax255": {"workload": "Allen-Cahn, 1 instance, lmax 255, 384x768, tf32x3, "
-                                        "256 steps forward + adjoint, checkpoints every 32",
-                            "steps_per_s": 256 / a4_s, "finite": a4_ok},
-                "schnakenberg_lmax511": {"workload": "Schnakenberg, 64 instances, lmax 511, 768x1536, "
-                                        "tf32x3, 64 steps forward + adjoint, checkpoints every 32, "
-                                        "gradients w.r.t. (a, b, D1, D2, dt) and the state",
-                            "instance_steps_per_s": 64 * 64 / a5_s, "finite": a5_ok},
-                "note": "wall-clock around ts_model_forward_backward (host round trips "
-                        "of the cotangents included)"},
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": sampler.summary(),
+            "plain_fp32": {"value": plain_pairs, "unit": "SHT pairs/s", "stage_ms": plain_stage},
+            "brusselator_sweep_lmax127": c3,
+            "adjoint": {
+                "allencahn_lmax255": {"workload": "Allen-Cahn, 1 instance, lmax 255, 384x768, tf32x3, "
+                                        "1000 steps forward + adjoint, checkpoints every 32",
+                            "steps_per_s": 1000 / a4_s, "finite": a4_ok},
+                "schnakenberg_lmax511": {"workload": "Schnakenberg, 64 instances, lmax 511, 768x1536, "
+                                        "tf32x3, 500 steps forward + adjoint, checkpoints every 32, "
+                                        "gradients w.r.t. (a, b, D1, D2, dt) and the state",
+                            "instance_steps_per_s": 64 * 500 / a5_s, "finite": a5_ok},
+                "note": "wall-clock around ts_model_forward_backward (host round trips "
+                        "of the cotangents included)"},
+            "schnakenberg_lmax511_forward": c5,
             "round_trip_rel_l2": rt,
             "flop_per_pair": flop_per_pair(lmax, lmax, nlat, nphi),
             "bytes_per_pair": bytes_per_pair(lmax, lmax, nlat, nphi),
+            # the metric's IMEX half and both ratios last, where a tail of the line shows them
+            "imex": {"model": "schnakenberg (2 species), D1 sweep", "instances": ni,
+                     "grid": f"lmax {lmax}, {nlat}x{nphi}", "launches_per_step": imex_launches,
+                     "single_lmax63": {"workload": "1 Schnakenberg instance, lmax 63, 96x192, "
+                                             "2000 steps as captured step graphs",
+                                 "fp32_steps_per_s": c1_fp32, "tc_steps_per_s": c1_tc},
+                     "finite": ok_tc and ok_fp,
+                     "tc_ms_per_step": imex_tc_ms / args.imex_steps,
+                     "fp32_ms_per_step": imex_fp_ms / kfp,
+                     "tc_steps_per_s_per_instance": args.imex_steps / (imex_tc_ms / 1e3),
+                     "unit": "instance-steps/s",
+                     "tc_steps_per_s": tc_imex, "fp32_steps_per_s": fp_imex,
+                     "tc_vs_fp32": tc_imex / fp_imex},
+            "sht_pairs": {"tc_pairs_per_s": value, "fp32_pairs_per_s": plain_pairs,
+                          "tc_vs_fp32": value / plain_pairs},
+            "imex_tc_vs_fp32": tc_imex / fp_imex,
         }
-        line["imex"]["tc_vs_fp32"] = line["imex"]["tc_steps_per_s"] / line["imex"]["fp32_steps_per_s"]
-        line["tc_vs_plain_sht"] = value / line["plain_fp32"]["value"]
         print(json.dumps(line), flush=True)
     return finish(plan, plain, dev, world)
+
+
+def workload_config(lmax, nlat, nphi, B, world):
+    """The `config` object, the same in both arms' lines."""
+    return {"workload": f"batched SHT round trip (synth+analys), lmax=mmax={lmax}, "
+                        f"{nlat}x{nphi} Gauss grid, B={B} fields per GPU",
+            "global_batch": B * world,
+            "l2": f"inputs larger than L2 (grid fields {4.0 * nlat * nphi * B / 1e6:.0f} MB/step)"}
+
+
+def pair_roofline(ms_per_step, B, bytes_pair, hbm, of):
+    """Roofline of the whole SHT pair: the minimum HBM bytes of one synth +
+    one analys per field (coefficients and grid, read and written, both
+    directions: 2 (8 nlm + 4 nlat nphi)) times the batch, over the device
+    time of one pair of batches."""
+    alg = bytes_pair * B
+    ach = alg / (ms_per_step / 1e3) / 1e9
+    return {"kernel": "SHT pair: all kernels of synth_dev + analys_dev", "bound": "hbm",
+            "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "peak_source": f"hbm_gbs ({of})", "algorithmic_bytes": alg}
+
+
+def profiled_pair_traffic(stages):
+    """DRAM bytes of one SHT pair (every stage's kernels, one launch each)
+    from the committed ncu summary, or None if a stage is missing."""
+    total = 0.0
+    for st in stages:
+        t = profiled_traffic(st)
+        if t is None:
+            return None
+        total += t
+    return total
+
+
+def time_forward_lmax511(dev, stream, ni=64, K=20):
+    """The lmax-511 inverse-problem workload's forward step (64 Schnakenberg
+    instances, 768 x 1536) on the tensor-core and on the plain FP32 plan
+    (CUDA events, K steps each), with each plan's synthesis error against the
+    f64 oracle on one seeded field: the comparison at the stated error."""
+    from oracle import oracle as O
+    from turing_sphere_b200 import ShtConfig, ShtPlan
+    lmax, nlat, nphi = 511, 768, 1536
+    out = {"workload": f"Schnakenberg, {ni} instances, lmax {lmax}, {nlat}x{nphi}, forward "
+                       f"IMEX steps ({K} timed per plan)"}
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    q = spectrum(lmax, 5)
+    want = ref.synth(q.astype(np.float64))
+    for prec in ("tf32x3", "fp32"):
+        plan = ShtPlan.create(dev, ShtConfig(lmax, lmax, nlat, nphi), {"precision": prec})
+        ms, launches, ok = time_imex(dev, plan, ni, K, 3, stream)
+        out[prec] = {"instance_steps_per_s": ni * K / (ms / 1e3), "ms_per_step": ms / K,
+                     "launches_per_step": launches, "finite": ok,
+                     "synth_rel_l2_vs_f64": float(np.sqrt(((plan.synth(q) - want) ** 2).sum()
+                                                          / (want ** 2).sum()))}
+        plan.destroy()
+    out["tc_vs_fp32"] = out["tf32x3"]["instance_steps_per_s"] / out["fp32"]["instance_steps_per_s"]
+    prof = profiled_kernels(PROFILE_511)
+    if prof:
+        out["ncu"] = prof
+    return out
+
+
+PROFILE_511 = os.path.join(ROOT, "profiles", "imex_schnakenberg_lmax511_i16_kernels.txt")
+
+
+def profiled_kernels(path):
+    """Per-kernel DRAM GB/s and tensor-pipe activity from a committed ncu
+    summary (lines 'kernel <name> time_us T ... dram_gbs G ... tensor_pct P'),
+    or None when the summary is absent."""
+    if not os.path.exists(path):
+        return None
+    out = {}
+    with open(path) as fh:
+        for line in fh:
+            if not line.startswith("kernel "):
+                continue
+            name = line[len("kernel "):line.index(" time_us")]
+            f = line.split()
+            row = {}
+            for key in ("time_us", "dram_gbs", "tensor_pct"):
+                if key in f:
+                    row[key] = float(f[f.index(key) + 1])
+            out[name.split("(")[0]] = row
+    return {"source": os.path.relpath(path, ROOT), "kernels": out}
 
 
 def finish(plan, plain, dev, world):

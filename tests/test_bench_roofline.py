@@ -20,3 +20,26 @@ def test_tensor_bound_when_the_flops_dominate():
 def test_fourier_stage_is_hbm():
     r = bench.stage_roofline("fourSynth", 0.128, 503e6, 6.47e9, 3, 6650.0, 1590.0, "of fallback")
     assert r["bound"] == "hbm" and "tensor_floor_us" not in r
+
+
+def test_whole_pair_roofline_uses_the_algorithmic_pair_bytes():
+    # lmax 255: 2.886 MB per pair, 256 pairs in 0.45 ms
+    from turing_sphere_b200.sht import bytes_per_pair
+    bpp = bytes_per_pair(255, 255, 384, 768)
+    assert abs(bpp - 2.886e6) < 1e3
+    r = bench.pair_roofline(0.45, 256, bpp, 6560.6, "of measured")
+    assert r["bound"] == "hbm" and abs(r["achieved"] - bpp * 256 / 0.45e-3 / 1e9) < 1e-6
+    assert abs(r["frac"] - r["achieved"] / 6560.6) < 1e-12
+
+
+def test_both_arms_print_the_same_config():
+    a = bench.workload_config(255, 384, 768, 256, 1)
+    assert a == bench.workload_config(255, 384, 768, 256, 1)
+    assert set(a) == {"workload", "global_batch", "l2"}
+
+
+def test_profiled_pair_traffic_sums_every_stage():
+    stages = ["legSynth", "fourSynth", "fourAnalysW", "legAnalysW"]
+    total = bench.profiled_pair_traffic(stages)
+    if total is not None:
+        assert total == sum(bench.profiled_traffic(s) for s in stages)
