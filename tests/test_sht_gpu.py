@@ -334,3 +334,27 @@ def test_second_device_in_the_same_process(device):
     assert O.rel_l2(back, q) < 1e-3
     plan.destroy()
     dev1.destroy()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
+@pytest.mark.parametrize("lmax,nlat,nphi", [(63, 96, 192), (127, 192, 384), (255, 384, 768),
+                                            (511, 768, 1536)])
+def test_second_fft_split(device, monkeypatch, precision, lmax, nlat, nphi):
+    """The FFT's second radix split (the one the autotuner may pick for these
+    row lengths; TS_FFT_ALT=1 selects it at plan creation): the plan reports
+    it, and a batch of synthesis + analysis stays within the transform bar of
+    the f64 oracle."""
+    monkeypatch.setenv("TS_FFT_ALT", "1")
+    alt = {192: (16, 6), 384: (24, 8), 768: (32, 12), 1536: (48, 16)}[nphi]
+    plan = make(device, lmax, nlat, nphi, precision=precision)
+    assert (plan.shapes["fft_p"], plan.shapes["fft_q"]) == alt
+    ref = O.ShtReference(lmax, lmax, nlat, nphi)
+    B = 3
+    qs = np.stack([scaled_spectrum(lmax, lmax, 80 + b) for b in range(B)])
+    sp = plan.synth(qs, batch=B).reshape(B, -1)
+    back = plan.analys(sp, batch=B).reshape(B, -1)
+    bar = TOL if (precision == "tf32x3" or lmax <= 255) else 6e-5
+    for b in (0, B - 1):
+        s_cpu = ref.synth(qs[b].astype(np.float64))
+        assert O.rel_l2(sp[b], s_cpu) < bar
+        assert O.rel_l2(back[b], ref.analys(sp[b].astype(np.float64))) < bar

@@ -2,8 +2,9 @@
 //
 // The shapes that decide a plan's speed depend on the grid and the GPU: the
 // tensor-core tiles (latitudes per synthesis tile, degrees per analysis
-// tile: operand reuse against pipeline depth and tile count) and the rows
-// per FFT CTA (occupancy against shared memory).  With TS_PLAN_AUTOTUNE the
+// tile: operand reuse against pipeline depth and tile count), the FFT's
+// radix split H = P*Q (the in-register DFT lengths of its two phases) and
+// its rows per CTA (occupancy against shared memory).  With TS_PLAN_AUTOTUNE the
 // plan times every candidate on a scratch batch at creation, keeps the
 // fastest, and remembers the choice for later plans of the same grid on the
 // same kind of device in this process.  The scratch batch holds zeros: the
@@ -18,6 +19,7 @@ namespace {
 
 struct Shapes {
   int nl = 0, ltl = 0, rows = 0;
+  bool alt = false;  // the FFT's second P*Q split
 };
 
 std::mutex g_mu;
@@ -71,6 +73,7 @@ void ts_autotune(ts_plan p) {
       p->tune_nl = it->second.nl;
       p->tune_ltl = it->second.ltl;
       p->fft_rows = it->second.rows;
+      p->fft_alt = it->second.alt;
       if (tc_changes) {
         ts_tc_free(p);
         ts_tc_init(p);
@@ -132,12 +135,16 @@ void ts_autotune(ts_plan p) {
       ts_tc_init(p);
     }
   }
-  // rows per FFT CTA
+  // FFT: the P*Q split (the default, and the second one where the row
+  // length has one) and the rows per CTA of each
   int P, Q;
   if (ts_f2_shape(p, &P, &Q)) {
     float best_ms = 1e30f;
-    int rows_seen[2] = {0, 0}, n = 0;
-    for (int rows : {8, 16, 4}) {
+    const bool has_alt = ts_f2_has_alt(p);
+    for (int alt = 0; alt <= (has_alt ? 1 : 0); alt++) {
+     p->fft_alt = alt != 0;
+     int rows_seen[2] = {0, 0}, n = 0;
+     for (int rows : {8, 16, 4}) {
       p->fft_rows = rows;
       const int r = ts_f2_rows(p);
       if (r == rows_seen[0] || r == rows_seen[1] || n == 2) continue;
@@ -155,9 +162,12 @@ void ts_autotune(ts_plan p) {
       if (ms < best_ms) {
         best_ms = ms;
         best.rows = r;
+        best.alt = alt != 0;
       }
+     }
     }
     p->fft_rows = best.rows;
+    p->fft_alt = best.alt;
   }
   TS_CUDA(cudaStreamSynchronize(s));
   p->tuned = true;

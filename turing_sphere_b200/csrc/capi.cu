@@ -426,6 +426,9 @@ int ts_sht_plan_create(ts_ctx ctx, int lmax, int mmax, int nlat, int nphi, int f
     if (p->precision == TS_PREC_BF16X3)
       ts_throw(TS_ERR_UNSUPPORTED, "split-BF16 tensor-core Legendre is not built; use TF32x3");
     if (p->precision == TS_PREC_TF32X3) ts_tc_init(p);
+    // TS_FFT_ALT=1 selects the FFT's second split where the row length has
+    // one (what the autotuner may also choose)
+    if (const char *e = getenv("TS_FFT_ALT")) p->fft_alt = atoi(e) != 0 && ts_f2_has_alt(p);
     if (flags & TS_PLAN_AUTOTUNE) ts_autotune(p);
     *out = p;
     return TS_OK;

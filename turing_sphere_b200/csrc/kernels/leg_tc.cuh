@@ -223,8 +223,15 @@ struct TsTcPipe {
 // of [north|south][16 latitudes][re, im] (68 floats per row keeps rows
 // 16-byte aligned); the analysis keeps [l][re|im] rows of 64 fields padded to
 // 65 floats, so that lanes reading different rows hit different banks
-#define TS_TC_SYN_ROW 68
-#define TS_TC_SYN_STAGING (TS_TC_FIELDS * TS_TC_SYN_ROW * 4)  // per epilogue group
+#define TS_TC_SYN_ROW 64
+#define TS_TC_SYN_STAGING (TS_TC_FIELDS * TS_TC_SYN_ROW * 4)  // per epilogue group: 16 KB
+// float index of value c (0..63) of field row fl in the synthesis staging of
+// the plain-store path: 16-byte chunks XOR (fl mod 8), so the 16 rows a warp
+// writes at once spread over 8 bank groups (a 64-float row pitch alone would
+// put them all in one)
+TS_DEV int ts_syn_stg(int fl, int c) {
+  return fl * TS_TC_SYN_ROW + ((((c >> 2) ^ (fl & 7)) << 2) | (c & 3));
+}
 #define TS_TC_ANA_ROW (TS_TC_FIELDS + 1)
 #define TS_TC_ANA_COLS 32  // accumulator columns an analysis group stages at a time
 
@@ -561,7 +568,6 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
     sc.decode(tile, m, lt, fb);
     sc.nch(m, n0, n1);
     const int et = ts_epi_row(warp, lane);  // 0..127 = TMEM lane = 2*field + comp
-    float *mine = sE + (et >> 1) * TS_TC_SYN_ROW + (et & 1);
     const unsigned lanebase = tbase + ((unsigned)((warp & 3) * 32) << 16);
     const bool zero = sc.stages(tile) == 0;  // a polar tile: no MMAs ran
     for (int c0 = 16 * grp; c0 < NL; c0 += 32) {
@@ -603,16 +609,15 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
       }
 #pragma unroll
       for (int i = 0; i < 16; i++) {
-        mine[2 * i] = e[i] + o[i];
-        mine[32 + 2 * i] = e[i] - o[i];
+        sE[ts_syn_stg(et >> 1, 2 * i + (et & 1))] = e[i] + o[i];
+        sE[ts_syn_stg(et >> 1, 32 + 2 * i + (et & 1))] = e[i] - o[i];
       }
       ts_epi_bar(grp);
 #pragma unroll 2
       for (int k = 0; k < 8; k++) {
         const int q = et + 128 * k, seg = q >> 3, part = q & 7;
         const int fl = seg >> 1, ns = seg & 1;
-        const float4 v =
-            *reinterpret_cast<const float4 *>(sE + fl * TS_TC_SYN_ROW + ns * 32 + part * 4);
+        const float4 v = *reinterpret_cast<const float4 *>(sE + ts_syn_stg(fl, ns * 32 + part * 4));
         const int f = fb * TS_TC_FIELDS + fl;
         const int lat = lt * NL + c0 + 2 * part;
         if (f >= nfields || lat >= t.nh) continue;

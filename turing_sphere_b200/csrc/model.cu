@@ -496,7 +496,7 @@ void schedule(ts_model m, Program &P, bool is_step) {
       // two-phase FFT when the row length has a shape and the row blocks fit
       int fP = 0, fQ = 0, fR = 0;
       const int nb = std::max<int>({(int)S.size(), (int)A.size(), 1});
-      if (ts_f2_shape(p, &fP, &fQ)) fR = ts_f2_phase_rows(p, nb, m->batch, &st.smem);
+      if (ts_f2_phase_shape(p, &fP, &fQ)) fR = ts_f2_phase_rows(p, nb, m->batch, &st.smem);
       const bool tcw = p->precision != TS_PREC_FP32 && fR && !A.empty();
       if (fR) {
         st.expr = "ts_f2_phase<" + pn + ", " + std::to_string(fP) + ", " + std::to_string(fQ) +

@@ -116,6 +116,8 @@ struct ts_plan_s {
   void *tc = nullptr;
   // kernel shapes: 0 = default (or TS_TC_NL / TS_TC_LTL); set by the autotuner
   int tune_nl = 0, tune_ltl = 0, fft_rows = 0;
+  // the FFT's second P*Q split (TS_F2_ALT_SHAPES) instead of the default one
+  bool fft_alt = false;
   bool tuned = false;
 };
 
@@ -158,6 +160,10 @@ int ts_fourier_lb(ts_plan p, int nblocks_y, int nrows, size_t *smem);
 // two-phase FFT (kernels/fft2.cuh): the plan's shape H = P*Q (false: none,
 // the Stockham kernels run), its shared memory, and the rows of a phase CTA
 bool ts_f2_shape(ts_plan p, int *P, int *Q);
+// the split of the fused grid phase (always the default), and whether the
+// plan's row length has a second split for the standalone FFTs
+bool ts_f2_phase_shape(ts_plan p, int *P, int *Q);
+bool ts_f2_has_alt(ts_plan p);
 size_t ts_f2_bytes(int P, int Q, int R, int nb);
 int ts_f2_phase_rows(ts_plan p, int nb, int batch, size_t *smem);
 // raise a kernel's dynamic shared-memory limit on `device` (once per size)

@@ -408,8 +408,57 @@ void ts_launch_leg_analys(ts_plan p, const float2 *g, long gs, float2 *q, long q
   X(1024, 32, 32, 8, 16) \
   X(1536, 48, 32, 4, 8)
 
+// The second split the autotuner tries for the grids of the transform
+// workloads (nphi = 192, 384, 768, 1536): a longer DFT in the second phase,
+// fewer rows in flight per thread block.  The fused grid phase always runs
+// the default split (its registers hold every species' P points).
+#define TS_F2_ALT_SHAPES(X) \
+  X(96, 16, 6, 8, 16)       \
+  X(192, 24, 8, 8, 16)      \
+  X(384, 32, 12, 8, 16)     \
+  X(768, 48, 16, 4, 8)
+
+bool ts_f2_has_alt(ts_plan p) {
+  if (p->fourier != TS_FOURIER_FFT) return false;
+  switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rlo, rhi) \
+  case h:                               \
+    return true;
+    TS_F2_ALT_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+    default:
+      return false;
+  }
+}
+
+bool ts_f2_phase_shape(ts_plan p, int *P, int *Q) {
+  if (p->fourier != TS_FOURIER_FFT) return false;
+  switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rlo, rhi) \
+  case h:                               \
+    *P = pp;                            \
+    *Q = qq;                            \
+    return true;
+    TS_F2_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+    default:
+      return false;
+  }
+}
+
 bool ts_f2_shape(ts_plan p, int *P, int *Q) {
   if (p->fourier != TS_FOURIER_FFT) return false;
+  if (p->fft_alt) switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rlo, rhi) \
+  case h:                               \
+    *P = pp;                            \
+    *Q = qq;                            \
+    return true;
+      TS_F2_ALT_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+      default:
+        break;
+    }
   switch (p->fft.H) {
 #define TS_F2_CASE(h, pp, qq, rlo, rhi) \
   case h:                               \
@@ -432,7 +481,7 @@ size_t ts_f2_bytes(int P, int Q, int R, int nb) {
 // and still gives every SM a CTA for `batch` instances (0: none fits)
 int ts_f2_phase_rows(ts_plan p, int nb, int batch, size_t *smem) {
   int P, Q;
-  if (!ts_f2_shape(p, &P, &Q)) return 0;
+  if (!ts_f2_phase_shape(p, &P, &Q)) return 0;
   const size_t cap = p->ctx->smem_optin;
   int want = 0;  // TS_PHASE_ROWS (16, 8 or 4) tunes it, like the reference's SHT_* knobs
   if (const char *e = getenv("TS_PHASE_ROWS")) want = atoi(e);
@@ -501,6 +550,15 @@ int pick_rows(ts_plan p, int nf, int rlo, int rhi) {
 
 int ts_f2_rows(ts_plan p) {
   if (p->fourier != TS_FOURIER_FFT) return 0;
+  if (p->fft_alt) switch (p->fft.H) {
+#define TS_F2_CASE(h, pp, qq, rlo, rhi) \
+  case h:                               \
+    return p->fft_rows == rlo ? rlo : rhi;
+      TS_F2_ALT_SHAPES(TS_F2_CASE)
+#undef TS_F2_CASE
+      default:
+        break;
+    }
   switch (p->fft.H) {
 #define TS_F2_CASE(h, pp, qq, rlo, rhi) \
   case h:                               \
@@ -515,7 +573,6 @@ int ts_f2_rows(ts_plan p) {
 bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, int fpb,
                                 char *wimg, cudaStream_t s) {
   if (p->fourier != TS_FOURIER_FFT) return false;
-  switch (p->fft.H) {
 #define TS_F2_CASE(h, pp, qq, rlo, rhi)                                     \
   case h:                                                                   \
     if (pick_rows(p, nf, rlo, rhi) == rlo)                                  \
@@ -523,6 +580,12 @@ bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, i
     else                                                                    \
       f2_analys_w<pp, qq, rhi>(p, spat, ss, nf, fpb, wimg, s);              \
     return true;
+  if (p->fft_alt) switch (p->fft.H) {
+      TS_F2_ALT_SHAPES(TS_F2_CASE)
+      default:
+        break;
+    }
+  switch (p->fft.H) {
     TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
     default:
@@ -533,11 +596,16 @@ bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, i
 void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, long ss, int nf,
                              cudaStream_t s) {
   if (p->fourier == TS_FOURIER_FFT) {
-    switch (p->fft.H) {
 #define TS_F2_CASE(h, pp, qq, rlo, rhi)                                         \
   case h:                                                                       \
     return pick_rows(p, nf, rlo, rhi) == rlo ? f2_synth<pp, qq, rlo>(p, fm, fs, spat, ss, nf, s) \
                               : f2_synth<pp, qq, rhi>(p, fm, fs, spat, ss, nf, s);
+    if (p->fft_alt) switch (p->fft.H) {
+        TS_F2_ALT_SHAPES(TS_F2_CASE)
+        default:
+          break;
+      }
+    switch (p->fft.H) {
       TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
       default:
@@ -560,11 +628,16 @@ void ts_launch_fourier_synth(ts_plan p, const float2 *fm, long fs, float *spat, 
 void ts_launch_fourier_analys(ts_plan p, const float *spat, long ss, float2 *g, long gs, int nf,
                               cudaStream_t s) {
   if (p->fourier == TS_FOURIER_FFT) {
-    switch (p->fft.H) {
 #define TS_F2_CASE(h, pp, qq, rlo, rhi)                                        \
   case h:                                                                      \
     return pick_rows(p, nf, rlo, rhi) == rlo ? f2_analys<pp, qq, rlo>(p, spat, ss, g, gs, nf, s) \
                               : f2_analys<pp, qq, rhi>(p, spat, ss, g, gs, nf, s);
+    if (p->fft_alt) switch (p->fft.H) {
+        TS_F2_ALT_SHAPES(TS_F2_CASE)
+        default:
+          break;
+      }
+    switch (p->fft.H) {
       TS_F2_SHAPES(TS_F2_CASE)
 #undef TS_F2_CASE
       default:
