@@ -51,3 +51,44 @@ def test_null_handles_are_rejected():
     assert L.ts_ctx_destroy(None) == _lib.TS_ERR_INVALID
     assert L.ts_sht_plan_destroy(None) == _lib.TS_ERR_INVALID
     assert L.ts_sht_synth_dev(None, None, None, 1, None) == _lib.TS_ERR_INVALID
+
+
+CONTEXT_CHECK = r"""
+import ctypes as C, sys
+sys.path.insert(0, sys.argv[1])
+from cuda.bindings import driver as cu
+from turing_sphere_b200 import _lib
+L = _lib.lib()
+def current():
+    err, ctx = cu.cuCtxGetCurrent()
+    assert err == cu.CUresult.CUDA_SUCCESS, err
+    return int(ctx)
+cu.cuInit(0)
+assert current() == 0  # this thread has never made a context current
+h, p = C.c_void_p(), C.c_void_p()
+assert L.ts_ctx_create(0, C.byref(h)) == 0
+assert current() == 0, "ts_ctx_create left a context current"
+assert L.ts_sht_plan_create(h, 15, 15, 16, 32, 0, C.byref(p)) == 0
+assert current() == 0, "ts_sht_plan_create left a context current"
+assert L.ts_sht_plan_destroy(p) == 0 and L.ts_ctx_destroy(h) == 0
+assert current() == 0
+print("ok")
+"""
+
+
+@pytest.mark.gpu
+def test_calls_leave_the_callers_context_as_they_found_it(tmp_path):
+    """Every C-ABI call makes its device current and gives the thread back the
+    context it had: a thread that never touched CUDA has no current context
+    after creating a context and a plan through the library (checked through
+    the driver API in a fresh process)."""
+    import subprocess
+    import sys
+    from tests.conftest import HAS_GPU
+    if not HAS_GPU:
+        pytest.skip("no CUDA device")
+    script = tmp_path / "ctx_check.py"
+    script.write_text(CONTEXT_CHECK)
+    r = subprocess.run([sys.executable, str(script), ROOT], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr

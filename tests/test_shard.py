@@ -123,7 +123,14 @@ def gpu_worker(rank, world, port, out):
                             timeout=datetime.timedelta(seconds=120))
     try:
         start, count = shard_range(N, rank, world)
-        full = gather_instances(gpu_run(list(range(start, start + count))), N)
+        # one GPU stands in for the ranks' GPUs here: the ranks take turns on it
+        # (in production each rank drives its own device)
+        local = None
+        for turn in range(world):
+            if turn == rank:
+                local = gpu_run(list(range(start, start + count)))
+            dist.barrier()
+        full = gather_instances(local, N)
         if rank == 0:
             np.save(out, full)
     finally:
@@ -134,10 +141,10 @@ def gpu_worker(rank, world, port, out):
 def test_two_rank_library_sweep_equals_unsharded(tmp_path):
     """The sharded path of the library itself: two ranks (gloo for the gather;
     both on GPU 0, each with its own CUDA context and its own block of a
-    5-instance Schnakenberg sweep, no kernel waiting on the other rank) run
-    their blocks through the C ABI; the gathered states match the f64 oracle
-    stepping each instance alone, and the unsharded batch run in this
-    process, instance by instance."""
+    5-instance Schnakenberg sweep, taking turns on the GPU) run their blocks
+    through the C ABI; the gathered states match the f64 oracle stepping each
+    instance alone, and the unsharded batch run in this process, instance by
+    instance."""
     from tests.conftest import HAS_GPU
     if not HAS_GPU:
         pytest.skip("no CUDA device")
@@ -166,6 +173,23 @@ def test_two_rank_library_sweep_equals_unsharded(tmp_path):
     assert full.shape == here.shape
     e_sharded = [O.rel_l2(full[k], want[k]) for k in range(N)]
     e_here = [O.rel_l2(here[k], want[k]) for k in range(N)]
-    assert max(e_sharded) < 1e-5 and max(e_here) < 1e-5, (e_sharded, e_here)
+    if max(e_sharded) >= 1e-5 or max(e_here) >= 1e-5:
+        # which neighbouring run each wrong row matches: one step fewer or
+        # more, or another instance's parameters
+        diag = {}
+        for k in range(N):
+            if e_sharded[k] < 1e-5:
+                continue
+            p = gpu_sweep(k)
+            st = np.stack(spectral_seed(GPU_LMAX, p, 1 + k)).astype(np.float64)
+            prm = [p[n] for n in ("a", "b", "D1", "D2", "dt")]
+            d = {f"steps{n}": O.rel_l2(full[k], ref.model_step("schnakenberg", prm, st, n)[0])
+                 for n in (GPU_STEPS - 1, GPU_STEPS + 1)}
+            for j in range(N):
+                q = gpu_sweep(j)
+                d[f"params{j}"] = O.rel_l2(full[k], ref.model_step(
+                    "schnakenberg", [q[n] for n in ("a", "b", "D1", "D2", "dt")], st, GPU_STEPS)[0])
+            diag[k] = d
+        raise AssertionError((e_sharded, e_here, diag))
     for k in range(N):
         assert O.rel_l2(full[k], here[k]) < 1e-6, k

@@ -135,6 +135,13 @@ void ts_set_error(ts_ctx ctx, const std::string &msg) {
     g_noctx_err = msg;
 }
 
+void ts_plan_take_timeout(ts_plan p) {
+  if (!ts_tc_check_error(p)) return;
+  int zero = 0;
+  TS_CUDA(cudaMemcpy(ts_tc_tab(p).err, &zero, sizeof(int), cudaMemcpyHostToDevice));
+  ts_throw(TS_ERR_TIMEOUT, "a tensor-core kernel gave up a bounded wait: its results are incomplete");
+}
+
 cudaStream_t ts_pick_stream(ts_ctx ctx, void *stream) {
   return stream ? (cudaStream_t)stream : ctx->stream;
 }
@@ -497,11 +504,7 @@ int ts_sht_plan_status(ts_plan p) {
   TS_REQUIRE(p != nullptr, TS_ERR_INVALID, "null plan");
   ts_device_guard dev_guard_(ctx->device);
   TS_CUDA(cudaStreamSynchronize(ctx->stream));
-  if (ts_tc_check_error(p)) {
-    int zero = 0;
-    TS_CUDA(cudaMemcpy(ts_tc_tab(p).err, &zero, sizeof(int), cudaMemcpyHostToDevice));
-    ts_throw(TS_ERR_TIMEOUT, "a tensor-core kernel gave up waiting for its MMAs");
-  }
+  ts_plan_take_timeout(p);
   TS_API_END(ctx)
 }
 

@@ -1782,6 +1782,8 @@ int ts_model_read(ts_model m, const char *name, float *out, long n) {
     TS_CUDA(cudaMemcpyAsync(out, ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
   }
   TS_CUDA(cudaStreamSynchronize(ctx->stream));
+  // values computed by a tensor-core kernel that gave up a wait are incomplete
+  ts_plan_take_timeout(p);
   TSM_END
 }
 

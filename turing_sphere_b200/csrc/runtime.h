@@ -218,4 +218,7 @@ bool ts_launch_fourier_analys_w(ts_plan p, const float *spat, long ss, int nf, i
                                 char *wimg, cudaStream_t s);
 // north/south pairs per CTA of the paired Fourier kernels, and their shared memory
 int ts_tc_check_error(ts_plan p);
+// after a synchronisation: TS_ERR_TIMEOUT (once; the flag is cleared) when a
+// tensor-core kernel of the plan gave up a bounded wait since the last check
+void ts_plan_take_timeout(ts_plan p);
 void ts_kernel_attrs_once(ts_ctx ctx);
