@@ -189,17 +189,23 @@ void require_len(const char *name, long got, long want) {
   ts_throw(TS_ERR_SIZE, buf);
 }
 
-// Fields per chunk of a host-array transform: a quarter of the batch, a
-// multiple of 16 fields, with at most 64 MB of the larger host array per
-// chunk (at lmax 255, 256 fields: 64-field chunks of the round trip's
-// coefficients measured 131 K pairs/s against 126-130 K for 16-32 and
-// 88-117 K for 128-256); a batch under 32 fields moves in one piece.
-// TS_HOST_CHUNK overrides it.
+// Fields per chunk of a host-array transform.  The pipeline ends one chunk's
+// transform and device->host copy after the last host->device copy, while a
+// chunk's transform has a fixed cost (tensor-core tiles of 64 fields) that
+// the copies must hide.  Fields of 192 KB or more (lmax >= 255) go 24 at a
+// time: on B200 (55 GB/s one way, 45 GB/s each way at once) the round trip
+// of 256 fields at lmax 255 measured 1.68 ms in chunks of 24 against 1.83
+// for 20, 1.84 for 28, 1.95 for 32 and 64, 2.07 for 16; 64 fields at lmax 511
+// 2.20 ms in chunks of 20-24 against 2.35 for 16 and 3.10 for 64.  Smaller
+// fields (lmax 63, 127: the fixed cost dominates) go a quarter of the batch
+// at a time, a multiple of 16 fields with at most 64 MB of the larger host
+// array, and a batch under 32 fields in one piece.  TS_HOST_CHUNK overrides it.
 int host_chunk(int batch, long floats_per_field) {
   if (const char *e = getenv("TS_HOST_CHUNK")) {
     const int c = atoi(e);
     if (c > 0) return std::min(c, batch);
   }
+  if (4 * floats_per_field >= (192L << 10)) return std::min(24, batch);
   if (batch < 32) return batch;
   long c = ((batch + 3) / 4 + 15) / 16 * 16;
   const long cap = std::max(16L, (64L << 20) / (4 * floats_per_field) / 16 * 16);
