@@ -307,7 +307,9 @@ int ts_model_describe(ts_model model, int which, char *buf, size_t cap);
 /* The generated CUDA C of both functions. */
 int ts_model_source(ts_model model, char *buf, size_t cap);
 /* Element-wise statements (the reference's kernel count, the fusion guard of
- * test/modelChecks.ts:17-21) and launches per call. */
+ * test/modelChecks.ts:17-21) and CUDA kernel launches per call (on a
+ * tensor-core plan a Legendre synthesis is two: the operand relayout and the
+ * tcgen05 contraction). */
 int ts_model_counts(ts_model model, int which, int *kernels, int *launches);
 
 /* Everything ts_model_compile does short of the GPU — parse, specialise,

@@ -1843,11 +1843,22 @@ int ts_model_source(ts_model m, char *buf, size_t cap) {
   TSM_END
 }
 
+namespace {
+// CUDA kernel launches of one call of a program: on a tensor-core plan a
+// Legendre synthesis stage is two (the operand relayout, then the tcgen05
+// contraction)
+int kernel_launches(ts_plan p, const Program &P) {
+  int n = 0;
+  for (auto &s : P.stages) n += s.kind == Stage::LegSynth && p->precision != TS_PREC_FP32 ? 2 : 1;
+  return n;
+}
+}  // namespace
+
 int ts_model_counts(ts_model m, int which, int *kernels, int *launches) {
   TSM_BEGIN(m)
   TS_REQUIRE(which == 0 || which == 1, TS_ERR_INVALID, "which: 0 = init, 1 = step");
   if (kernels) *kernels = tsm::count_kernels(m->prog[which].fn);
-  if (launches) *launches = (int)m->prog[which].stages.size();
+  if (launches) *launches = kernel_launches(m->plan, m->prog[which]);
   TSM_END
 }
 
@@ -1910,7 +1921,7 @@ int ts_model_check(int lmax, int mmax, int nlat, int nphi, const char *source,
                describe_program(mod.prog[1]).c_str());
     }
     if (kernels) *kernels = tsm::count_kernels(mod.prog[1].fn);
-    if (launches) *launches = (int)mod.prog[1].stages.size();
+    if (launches) *launches = kernel_launches(&plan, mod.prog[1]);
     return TS_OK;
   } catch (const ts_exc &e) {
     if (err && err->message[0] == 0) snprintf(err->message, sizeof err->message, "%s", e.msg.c_str());
