@@ -179,12 +179,12 @@ TS_DEV void ts_f2_rk(int tid, int &r, int &k1) {
   }
 }
 
-// twq[n2 (P+1) + k1] = w^{n2 k1}
+// twq[n2 (P+1) + k1] = w^{n2 k1} = tw[2 n2 k1] (2 n2 k1 <= 2 (P-1)(Q-1) < nphi)
 template <class C>
 TS_DEV void ts_f2_twq(float2 *twq, const TsFftTab &ft) {
   for (int i = threadIdx.x; i < C::Q * C::P; i += C::T) {
     const int n2 = i / C::P, k1 = i - n2 * C::P;
-    twq[n2 * C::P1 + k1] = __ldg(ft.tw + (2 * n2 * k1) % ft.nphi);
+    twq[n2 * C::P1 + k1] = __ldg(ft.tw + 2 * n2 * k1);
   }
 }
 
@@ -407,7 +407,10 @@ TS_DEV void ts_f2_forward_in(float2 *b, const float2 *twq, const float *__restri
 // of one field.  lat_of(r) < 0 marks a row without a latitude (zeros).
 // Item i is the pair (k, H-k), k = i / R, of row i % R: consecutive threads
 // read consecutive latitudes.  Every load of a thread is issued before the
-// first is used.
+// first is used.  One twiddle serves both members of a pair: with
+// s = X[k] + conj X[H-k] and u = i e^{2 pi i k/nphi} (X[k] - conj X[H-k]),
+// Z[k] = s + u and, as e^{2 pi i (H-k)/nphi} = -conj e^{2 pi i k/nphi},
+// Z[H-k] = conj(s - u).
 template <class C, class LatOf>
 TS_DEV void ts_f2_pack(float2 *b, const float2 *__restrict__ src, const TsFftTab &ft,
                        LatOf lat_of) {
@@ -435,23 +438,30 @@ TS_DEV void ts_f2_pack(float2 *b, const float2 *__restrict__ src, const TsFftTab
       const int h = H - kk;
       const float2 x = kk == 0 ? make_float2(xk[j].x, 0.f) : xk[j];
       const float2 ch = c_conj(xh[j]);
-      row[kk] = c_add(c_add(x, ch), c_mul_i(c_mul(c_sub(x, ch), __ldg(ft.tw + kk))));
-      if (kk > 0 && kk < h) {
-        const float2 ck = c_conj(x);
-        row[h] = c_add(c_add(xh[j], ck), c_mul_i(c_mul(c_sub(xh[j], ck), __ldg(ft.tw + h))));
-      }
+      const float2 sp = c_add(x, ch);
+      const float2 u = c_mul_i(c_mul(c_sub(x, ch), __ldg(ft.tw + kk)));
+      row[kk] = c_add(sp, u);
+      if (kk > 0 && kk < h) row[h] = c_conj(c_sub(sp, u));
     }
   }
+}
+
+// 2 X[k] of the analysis from the forward-transformed row and the twiddle
+// t = e^{2 pi i k/nphi}: with a = Z[k], b = conj Z[H-k],
+// 2 X[k] = (a + b) - i conj(t) (a - b)
+template <class C>
+TS_DEV float2 ts_f2_xk2(const float2 *row, int k, float2 t) {
+  const float2 zk = row[k];
+  const float2 zh = c_conj(row[k == 0 ? 0 : C::H - k]);
+  const float2 sm = c_add(zk, zh), d = c_sub(zk, zh);
+  // -i conj(t) d = (d.y t.x - d.x t.y, -(d.x t.x + d.y t.y))
+  return make_float2(sm.x + (d.y * t.x - d.x * t.y), sm.y - (d.x * t.x + d.y * t.y));
 }
 
 // X[k] of the analysis from the forward-transformed row
 template <class C>
 TS_DEV float2 ts_f2_xk(const float2 *row, int k, const TsFftTab &ft) {
-  const float2 zk = row[k];
-  const float2 zh = c_conj(row[k == 0 ? 0 : C::H - k]);
-  const float2 xe = c_scale(c_add(zk, zh), 0.5f);
-  const float2 xo = c_mul_negi(c_scale(c_sub(zk, zh), 0.5f));
-  return c_add(xe, c_mul(xo, c_conj(__ldg(ft.tw + k))));
+  return c_scale(ts_f2_xk2<C>(row, k, __ldg(ft.tw + k)), 0.5f);
 }
 
 // X[k], k <= mmax, of the CTA's rows -> dst[k*nlat + lat]
@@ -531,7 +541,7 @@ TS_DEV void ts_f2_write_w(const float2 *b, int lat0, long f, const TsFftTab &ft,
   if (lat >= nh) return;
   const float2 *rn = b + j * C::RP, *rs = b + (NPR + j) * C::RP;
   const bool south = ft.nlat - 1 - lat != lat;
-  const float w = __ldg(wq + lat);
+  const float w = 0.5f * __ldg(wq + lat);  // times 2 X[k] of both rows
   // byte offsets of (row 2 fl + re|im, column lat % 32) inside a 16 KB block,
   // and of this field block's chunk: block (((k nfb + fb) 2 + par) nlc + lat / 32)
   const int o_re = ts_swz_img(2 * fl, lat & 31), o_im = ts_swz_img(2 * fl + 1, lat & 31);
@@ -547,8 +557,9 @@ TS_DEV void ts_f2_write_w(const float2 *b, int lat0, long f, const TsFftTab &ft,
   const int kend = min(ft.mmax + 1, max(kl0, kl1));
   for (int k = k0; k < kend; k += 2 * C::P) {
     const bool e0 = k < kl0, e1 = k < kl1;
-    const float2 xn = ts_f2_xk<C>(rn, k, ft);
-    const float2 xs = south ? ts_f2_xk<C>(rs, k, ft) : make_float2(0.f, 0.f);
+    const float2 t = __ldg(ft.tw + k);
+    const float2 xn = ts_f2_xk2<C>(rn, k, t);
+    const float2 xs = south ? ts_f2_xk2<C>(rs, k, t) : make_float2(0.f, 0.f);
     char *blk = base + k * kstep;
     if (e0) {
       *reinterpret_cast<float *>(blk + o_re) = w * (xn.x + xs.x);
