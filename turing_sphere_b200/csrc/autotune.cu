@@ -107,7 +107,7 @@ void ts_autotune(ts_plan p) {
     qf.nper = 1;
     float best_ms = 1e30f;
     std::vector<std::pair<int, int>> seen;
-    for (int nl : {64, 96, 128})
+    for (int nl : {64, 96})
       for (int ltl : {64, 128}) {
         p->tune_nl = nl;
         p->tune_ltl = ltl;

@@ -8,20 +8,27 @@
 //              W_0 = w (G_north + G_south), W_1 = w (G_north - G_south)
 // P comes from tables computed in FP64 on the GPU and stored as TF32 hi/lo
 // pairs, already in the shared-memory byte image the MMA reads (K-major,
-// 128-byte swizzle), so a CTA streams them with plain 16-byte copies.  The
+// 128-byte swizzle), so a CTA streams them with plain bulk copies.  The
 // data operand (Q or W) is split on the fly: hi = rna_tf32(x),
 // lo = rna_tf32(x - hi); each k-step issues hi*hi + hi*lo + lo*hi.
 //
 // Both operands reach shared memory by cp.async.bulk: the P table from its
 // precomputed image and the data operand from a raw-fp32 image of the same
 // byte layout (TsTcImg; written by a relayout kernel for the synthesis and by
-// the Fourier analysis itself for the analysis).  The kernels are persistent
+// the Fourier analysis itself for the analysis).  The split data operand then
+// lives in tensor memory: the MMAs read A (hi, lo) from TMEM and only B (the
+// table) from shared memory.  An MMA of 128 x N x 8 reading both operands from
+// shared memory needs (4 KB + N * 32 B) per 2 * 128 * N * 8 flops, more than
+// the shared-memory bandwidth at the TF32 rate for N = 96, with the copies,
+// the split and the epilogue staging competing for the same banks; with A in
+// TMEM a stage moves 40% fewer shared-memory bytes.  The kernels are persistent
 // (one CTA per SM walking tiles blockIdx.x + k*gridDim.x) with 448 threads in
-// fixed roles: warps 0-3 split each data tile in place into rna-rounded TF32
-// hi and lo, warp 4 issues the copies (expect-tx mbarriers over an S-slot
-// ring), warp 5 issues the MMAs, warps 6-13 drain the accumulators.  Tensor
-// memory holds two accumulator buffers, so the epilogue of tile i overlaps the
-// MMAs of tile i+1 and the operand ring streams across tile boundaries.
+// fixed roles: warps 0-3 split each data tile row by row (thread = row = TMEM
+// lane) into rna-rounded TF32 hi and lo in an NA-slot TMEM operand ring, warp 4
+// issues the copies (expect-tx mbarriers over an S-slot shared-memory ring),
+// warp 5 issues the MMAs, warps 6-13 drain the accumulators.  Tensor memory
+// holds two accumulator buffers, so the epilogue of tile i overlaps the MMAs
+// of tile i+1, and both operand rings stream across tile boundaries.
 // Every wait is bounded: on timeout the kernel records an error flag, waits
 // (bounded) for its copies and MMAs in flight, frees its tensor memory and
 // returns.
@@ -101,6 +108,17 @@ TS_DEV void ts_mma_tf32(unsigned dtmem, unsigned long long adesc, unsigned long 
       "r"(0));
 }
 
+// the same with A (128 lanes x 8 columns of tf32) read from tensor memory
+TS_DEV void ts_mma_tf32_ta(unsigned dtmem, unsigned atmem, unsigned long long bdesc,
+                           unsigned idesc, unsigned accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      ::"r"(dtmem), "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0),
+      "r"(0));
+}
+
 TS_DEV void ts_mma_commit(unsigned long long *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    ts_smem_u32(bar))
@@ -120,6 +138,22 @@ TS_DEV void ts_tmem_ld16(unsigned taddr, float (&v)[16]) {
 #pragma unroll
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
+
+// 16 consecutive columns of this thread's TMEM lane (warp-collective; taddr
+// is the warp's lane base plus the first column)
+TS_DEV void ts_tmem_st16(unsigned taddr, const float (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+TS_DEV void ts_tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 TS_DEV unsigned ts_tmem_cols(int n) {
   unsigned c = 32;
@@ -158,6 +192,8 @@ TS_DEV void ts_tma_store3(const TsTmaDesc *map, const void *src, int x, int y, i
 }
 TS_DEV void ts_bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 TS_DEV void ts_bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// all but the most recent bulk group have finished reading shared memory
+TS_DEV void ts_bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 TS_DEV void ts_bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // byte offset of element (row r, k) in a K-major 128B-swizzled tile whose
@@ -202,14 +238,18 @@ TS_DEV long ts_atile_offset(const TsTcTab &tc, int lmax, int m, int par, int lti
 
 #define TS_TC_THREADS 448  // 14 warps: split 0-3, copy 4, MMA 5, epilogue 6-13
 #define TS_TC_MAXSTAGE 4
+#define TS_TC_ASLOTS 4      // TMEM operand slots at most (64 columns each: hi | lo)
+#define TS_TC_STAGE_A 16384 // shared-memory bytes of a stage's raw data tile
 
-// Persistent pipeline state.  Operand ring: full[s] the copies of slot s
-// landed; ready[s] the 4 split warps converted its data tile; empty[s] the
-// MMAs that read it are done.  Accumulators (two TMEM buffers): acc_full[b]
-// the MMAs of a tile into buffer b are done; acc_empty[b] the epilogue warps
-// have read it out.
+// Persistent pipeline state.  Shared-memory ring: full[s] the copies of slot
+// s landed; empty[s] the MMAs that read its table are done.  TMEM operand
+// ring: a_full[a] the 4 split warps stored a data tile's hi/lo in slot a;
+// a_empty[a] the MMAs that read it are done.  Accumulators (two TMEM
+// buffers): acc_full[b] the MMAs of a tile into buffer b are done;
+// acc_empty[b] the epilogue warps have read it out.
 struct TsTcPipe {
-  unsigned long long full[TS_TC_MAXSTAGE], ready[TS_TC_MAXSTAGE], empty[TS_TC_MAXSTAGE];
+  unsigned long long full[TS_TC_MAXSTAGE], empty[TS_TC_MAXSTAGE];
+  unsigned long long a_full[TS_TC_ASLOTS], a_empty[TS_TC_ASLOTS];
   unsigned long long acc_full[2], acc_empty[2];
   unsigned long long epi;    // the 4 epilogue warps' own barrier
   unsigned long long drain;  // the MMA warp's last commit before exit
@@ -224,7 +264,8 @@ struct TsTcPipe {
 // 16-byte aligned); the analysis keeps [l][re|im] rows of 64 fields padded to
 // 65 floats, so that lanes reading different rows hit different banks
 #define TS_TC_SYN_ROW 64
-#define TS_TC_SYN_STAGING (TS_TC_FIELDS * TS_TC_SYN_ROW * 4)  // per epilogue group: 16 KB
+#define TS_TC_SYN_STAGING (TS_TC_FIELDS * TS_TC_SYN_ROW * 4)  // one staging buffer: 16 KB
+#define TS_TC_SYN_NSTG 2  // staging buffers per epilogue group, used in turn
 // float index of value c (0..63) of field row fl in the synthesis staging of
 // the plain-store path: 16-byte chunks XOR (fl mod 8), so the 16 rows a warp
 // writes at once spread over 8 bank groups (a 64-float row pitch alone would
@@ -259,8 +300,11 @@ TS_DEV void ts_tc_pipe_init(TsTcPipe *pp, int S, const TsTcTab &tc) {
     pp->limit = tc.wait_limit ? tc.wait_limit : TS_TC_WAIT_LIMIT;
     for (int s = 0; s < S; s++) {
       ts_mbar_init(&pp->full[s], 1);
-      ts_mbar_init(&pp->ready[s], 4);
       ts_mbar_init(&pp->empty[s], 1);
+    }
+    for (int a = 0; a < TS_TC_ASLOTS; a++) {
+      ts_mbar_init(&pp->a_full[a], 4);
+      ts_mbar_init(&pp->a_empty[a], 1);
     }
     for (int b = 0; b < 2; b++) {
       ts_mbar_init(&pp->acc_full[b], 1);
@@ -296,35 +340,44 @@ TS_DEV void ts_bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned lon
       : "memory");
 }
 
-// warps 0-3: split the raw fp32 tile at `ahi` in place into hi = rna_tf32(x)
-// and lo = rna_tf32(x - hi) at `alo` (element order is irrelevant: it is a
-// pure element-wise map over the 16 KB block)
-TS_DEV void ts_tc_split16k(char *ahi, char *alo, int tid) {
+// warps 0-3: row r (= tid, the TMEM lane of warp r/32) of the raw fp32 data
+// tile at `tile` (K-major, 128-byte swizzle, 32 values) split into
+// hi = rna_tf32(x) and lo = rna_tf32(x - hi), stored in TMEM columns
+// [col, col + 32) and [col + 32, col + 64) of the lane; `taddr` is the warp's
+// lane base plus col.  A warp reads each 16-byte chunk index of 32 rows: the
+// swizzle spreads every 8 rows over 8 distinct bank groups.
+TS_DEV void ts_tc_split_tmem(const char *tile, unsigned taddr, int r) {
+  const char *row = tile + (r >> 3) * 1024 + (r & 7) * 128;
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const int off = (tid + i * 128) * 16;
-    const float4 x = *reinterpret_cast<const float4 *>(ahi + off);
-    float4 h, l;
-    h.x = ts_rna_tf32(x.x);
-    h.y = ts_rna_tf32(x.y);
-    h.z = ts_rna_tf32(x.z);
-    h.w = ts_rna_tf32(x.w);
-    l.x = ts_rna_tf32(x.x - h.x);
-    l.y = ts_rna_tf32(x.y - h.y);
-    l.z = ts_rna_tf32(x.z - h.z);
-    l.w = ts_rna_tf32(x.w - h.w);
-    *reinterpret_cast<float4 *>(ahi + off) = h;
-    *reinterpret_cast<float4 *>(alo + off) = l;
+  for (int h = 0; h < 2; h++) {
+    float hi[16], lo[16];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const float4 x = *reinterpret_cast<const float4 *>(row + (((4 * h + c) ^ (r & 7)) << 4));
+      hi[4 * c + 0] = ts_rna_tf32(x.x);
+      hi[4 * c + 1] = ts_rna_tf32(x.y);
+      hi[4 * c + 2] = ts_rna_tf32(x.z);
+      hi[4 * c + 3] = ts_rna_tf32(x.w);
+      lo[4 * c + 0] = ts_rna_tf32(x.x - hi[4 * c + 0]);
+      lo[4 * c + 1] = ts_rna_tf32(x.y - hi[4 * c + 1]);
+      lo[4 * c + 2] = ts_rna_tf32(x.z - hi[4 * c + 2]);
+      lo[4 * c + 3] = ts_rna_tf32(x.w - hi[4 * c + 3]);
+    }
+    ts_tmem_st16(taddr + 16 * h, hi);
+    ts_tmem_st16(taddr + 32 + 16 * h, lo);
   }
 }
 
 // MMA issue (one thread): per tile, wait until the epilogue has drained the
-// accumulator buffer, then per stage wait for the split data tile, issue the
-// 3-pass products of its 4 k-steps and commit the slot back to the copy warp;
-// the tile's last commit signals the epilogue.
+// accumulator buffer, then per stage wait for the split data tile in TMEM
+// slot a (the split warps waited for the stage's copies, table included),
+// issue the 3-pass products of its 4 k-steps and commit the shared-memory slot
+// back to the copy warp and the TMEM slot back to the split warps; the tile's
+// last commit signals the epilogue.  TMEM columns: accumulator buffer b at
+// b * acc_cols, operand slot a at a_col0 + 64 a (hi, then lo).
 template <class Sched>
-TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes, unsigned tmem,
-                           int acc_cols, const Sched &sc) {
+TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, int NA, unsigned stage_bytes,
+                           unsigned tmem, int acc_cols, unsigned a_col0, const Sched &sc) {
   const int ntiles = sc.ntiles();
   long g = 0;
   int i = 0;
@@ -340,25 +393,26 @@ TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes
     const unsigned tb = sc.table_bytes(ti);
     const unsigned idesc = ts_idesc_tf32(sc.n(ti));
     for (int t_ = 0; t_ < T; t_++, g++) {
-      const int s = (int)(g % S);
-      const unsigned use = (unsigned)(g / S);
-      if (!ts_mbar_wait(&pp->ready[s], use & 1, pp->limit)) {
+      const int s = (int)(g % S), a = (int)(g % NA);
+      const unsigned ause = (unsigned)(g / NA);
+      if (!ts_mbar_wait(&pp->a_full[a], ause & 1, pp->limit)) {
         ts_tc_flag(pp);
         return;
       }
       ts_tc_fence_after();
-      const unsigned ahi = ts_smem_u32(smem + s * stage_bytes), alo = ahi + 16384;
-      const unsigned bhi = ahi + 2 * 16384, blo = bhi + tb / 2;
+      const unsigned bhi = ts_smem_u32(smem + s * stage_bytes) + TS_TC_STAGE_A, blo = bhi + tb / 2;
+      const unsigned ahi = tmem + a_col0 + 64u * (unsigned)a, alo = ahi + 32;
       const unsigned d = tmem + (unsigned)(b * acc_cols + sc.d_col(ti, t_));
       const bool init = sc.first(ti, t_);
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) {
         const unsigned acc = (!init || kk > 0) ? 1u : 0u;
-        ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, acc);
-        ts_mma_tf32(d, ts_umma_desc(ahi + kk * 32), ts_umma_desc(blo + kk * 32), idesc, 1u);
-        ts_mma_tf32(d, ts_umma_desc(alo + kk * 32), ts_umma_desc(bhi + kk * 32), idesc, 1u);
+        ts_mma_tf32_ta(d, ahi + kk * 8, ts_umma_desc(bhi + kk * 32), idesc, acc);
+        ts_mma_tf32_ta(d, ahi + kk * 8, ts_umma_desc(blo + kk * 32), idesc, 1u);
+        ts_mma_tf32_ta(d, alo + kk * 8, ts_umma_desc(bhi + kk * 32), idesc, 1u);
       }
       ts_mma_commit(&pp->empty[s]);
+      ts_mma_commit(&pp->a_empty[a]);
     }
     ts_mma_commit(&pp->acc_full[b]);
   }
@@ -369,29 +423,36 @@ TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes
 // bases, skip offsets, computed once per tile) and, per stage, the data
 // tile, the table chunk and the accumulator column; every role walks the
 // same sequence, so ring slots and barrier phases stay in step.  Warps 0-3
-// split data tiles, warp 4 copies, warp 5 issues MMAs, warps 6-13 drain the
-// accumulators through `epilogue(tile, tmem_cols_of_buffer)`.
+// split data tiles into the TMEM operand ring (NA slots of 64 columns from
+// a_col0), warp 4 copies, warp 5 issues MMAs, warps 6-13 drain the
+// accumulators through `epilogue(tile, tmem_cols_of_buffer)`.  A
+// shared-memory slot holds the raw data tile (TS_TC_STAGE_A bytes) and then
+// the table's hi and lo images.
 template <class Sched, class Epilogue>
-TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_bytes, unsigned tmem,
-                             int acc_cols, const Sched &sc, Epilogue epilogue) {
+TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, int NA, unsigned stage_bytes,
+                             unsigned tmem, int acc_cols, unsigned a_col0, const Sched &sc,
+                             Epilogue epilogue) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntiles = sc.ntiles();
   if (warp < 4) {
     long g = 0;
+    const unsigned lanebase = tmem + ((unsigned)(warp * 32) << 16) + a_col0;
     for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x) {
       const int T = sc.stages(tile);
       for (int t_ = 0; t_ < T; t_++, g++) {
-        const int s = (int)(g % S);
-        const unsigned use = (unsigned)(g / S);
-        if (!ts_mbar_wait(&pp->full[s], use & 1, pp->limit)) {
+        const int s = (int)(g % S), a = (int)(g % NA);
+        const unsigned use = (unsigned)(g / S), ause = (unsigned)(g / NA);
+        if (!ts_mbar_wait(&pp->full[s], use & 1, pp->limit) ||
+            (ause > 0 && !ts_mbar_wait(&pp->a_empty[a], (ause - 1) & 1, pp->limit))) {
           ts_tc_flag(pp);
           return;
         }
-        char *ahi = smem + s * stage_bytes;
-        ts_tc_split16k(ahi, ahi + 16384, tid);
-        ts_fence_proxy_async();
+        ts_tc_fence_after();  // the stores follow the MMAs that read the slot before
+        ts_tc_split_tmem(smem + s * stage_bytes, lanebase + 64u * (unsigned)a, tid);
+        ts_tmem_wait_st();
+        ts_tc_fence_before();
         __syncwarp();
-        if (lane == 0) ts_mbar_arrive(&pp->ready[s]);
+        if (lane == 0) ts_mbar_arrive(&pp->a_full[a]);
       }
     }
   } else if (warp == 4) {
@@ -410,9 +471,9 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
             break;
           }
           char *st = smem + s * stage_bytes;
-          ts_mbar_arrive_tx(&pp->full[s], 16384 + tb);
-          ts_bulk_g2s(st, sc.a_src(ti, t_), 16384, &pp->full[s]);
-          ts_bulk_g2s(st + 2 * 16384, sc.b_src(ti, t_), tb, &pp->full[s]);
+          ts_mbar_arrive_tx(&pp->full[s], TS_TC_STAGE_A + tb);
+          ts_bulk_g2s(st, sc.a_src(ti, t_), TS_TC_STAGE_A, &pp->full[s]);
+          ts_bulk_g2s(st + TS_TC_STAGE_A, sc.b_src(ti, t_), tb, &pp->full[s]);
         }
         if (t_ < T) break;
       }
@@ -425,7 +486,7 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, unsigned stage_byt
     }
   } else if (warp == 5) {
     if (lane == 0) {
-      ts_tc_mma_role(smem, pp, S, stage_bytes, tmem, acc_cols, sc);
+      ts_tc_mma_role(smem, pp, S, NA, stage_bytes, tmem, acc_cols, a_col0, sc);
       // every MMA this thread issued has finished before TMEM is released
       ts_mma_commit(&pp->drain);
       if (!ts_mbar_wait(&pp->drain, 0, pp->limit)) ts_tc_flag(pp);
@@ -530,8 +591,9 @@ struct TsSynthSched {
 };
 
 // grid = min(#SMs, tiles), block = 448, persistent.  Dynamic shared memory:
-// S*(2*16384 + 2*NL*128) + 2*TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe).
-// TMEM: two buffers of 2*NL columns.  With tma_ok, fmap maps fm as floats
+// S*(16384 + 2*NL*128) + 2*TS_TC_SYN_NSTG*TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe).
+// TMEM: two accumulator buffers of 2*NL columns, then (512 - 4*NL)/64 operand
+// slots (NL <= 96: at least two).  With tma_ok, fmap maps fm as floats
 // [field][m][2 nlat] with a (32, 1, 64) box in the 128-byte swizzle, and
 // whole 16-latitude chunks leave through tensor stores (one thread per
 // epilogue group issues them); other chunks, or tma_ok = 0, use plain stores.
@@ -543,8 +605,10 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
   char *smem = (char *)(((unsigned long long)ts_smem_st + 1023) & ~1023ull);
   const int NL = tc.NL;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const unsigned stage = 2 * 16384 + 2 * NL * 128;
-  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage + 2 * TS_TC_SYN_STAGING);
+  const unsigned stage = TS_TC_STAGE_A + 2 * NL * 128;
+  const int NA = min(TS_TC_ASLOTS, (512 - 4 * NL) / 64);
+  TsTcPipe *pp = reinterpret_cast<TsTcPipe *>(smem + S * stage +
+                                               2 * TS_TC_SYN_NSTG * TS_TC_SYN_STAGING);
   const TsSynthSched sc{&tc, t.lmax, t.mmax, q_nfb, NL, tc.nLT, qimg};
   ts_tc_pipe_init(pp, S, tc);
   if (warp == 0) ts_tmem_alloc(&pp->tmem, 512);
@@ -559,7 +623,10 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
   // a partial chunk as 16-byte runs of whole complex values written by the
   // 128 threads, north in latitude order and south mirrored
   const int grp = ts_epi_group(warp);
-  float *sE = reinterpret_cast<float *>(smem + S * stage + (grp > 0 ? TS_TC_SYN_STAGING : 0));
+  // the group's staging buffers, used in turn: a chunk is staged while the
+  // previous chunk's tensor stores still read the other buffer
+  char *sE0 = smem + S * stage + (grp > 0 ? TS_TC_SYN_NSTG * TS_TC_SYN_STAGING : 0);
+  int nstaged = 0;
   const bool elected = warp >= 6 && ((warp - 6) & 3) == 0 && lane == 0;  // one per epilogue group
   const bool vec = (t.nlat % 2 == 0) && (fm_stride % 2 == 0) &&
                    ((reinterpret_cast<unsigned long long>(fm) & 15) == 0);
@@ -583,8 +650,10 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
 #pragma unroll
           for (int i = 0; i < 16; i++) o[i] = 0.f;
       }
-      // the group's previous tensor stores have read the staging rows
-      if (elected) ts_bulk_wait_read();
+      // the tensor stores that read this staging buffer (two chunks ago) are done
+      float *sE = reinterpret_cast<float *>(sE0 + (nstaged & 1) * TS_TC_SYN_STAGING);
+      nstaged++;
+      if (elected) ts_bulk_wait_read1();
       ts_epi_bar(grp);
       const int lat0 = lt * NL + c0;
       if (tma_ok && lat0 + 16 <= t.nh) {
@@ -643,7 +712,7 @@ ts_leg_synth_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ qimg, int q_nfb
       ts_epi_bar(grp);
     }
   };
-  ts_tc_persistent(smem, pp, S, stage, tmem, 2 * NL, sc, epilogue);
+  ts_tc_persistent(smem, pp, S, NA, stage, tmem, 2 * NL, 4u * NL, sc, epilogue);
   if (elected) ts_bulk_wait_all();
   ts_tc_fence_before();
   __syncthreads();
@@ -706,9 +775,9 @@ struct TsAnalysSched {
 // grid = min(#SMs, tiles), block = 448, persistent.  Tiles with no l values
 // have no stages; their epilogue does nothing; tiles whose latitude chunks
 // the polar skip drops entirely write zeros.  Dynamic shared memory:
-// S*(2*16384 + 2*Nmax*128) + 2*min(Nmax, TS_TC_ANA_COLS)*2*TS_TC_ANA_ROW*4 + 1024
-// + sizeof(TsTcPipe).  TMEM:
-// two buffers of 256 columns.
+// S*(16384 + 2*Nmax*128) + 2*min(Nmax, TS_TC_ANA_COLS)*2*TS_TC_ANA_ROW*4 + 1024
+// + sizeof(TsTcPipe).  TMEM: two accumulator buffers of 128 columns, then four
+// operand slots of 64.
 template <class Epi>
 __global__ void __launch_bounds__(TS_TC_THREADS, 1)
 ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nfb, Epi epi,
@@ -716,7 +785,7 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
   extern __shared__ __align__(1024) char ts_smem_at[];
   char *smem = (char *)(((unsigned long long)ts_smem_at + 1023) & ~1023ull);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const unsigned stage = 2 * 16384 + 2 * nmax * 128;
+  const unsigned stage = TS_TC_STAGE_A + 2 * nmax * 128;
   const int grp = ts_epi_group(warp);
   const int ana_stg = min(nmax, TS_TC_ANA_COLS) * 2 * TS_TC_ANA_ROW * 4;  // bytes per group
   float *sD = reinterpret_cast<float *>(smem + S * stage + (grp > 0 ? ana_stg : 0));
@@ -765,7 +834,7 @@ ts_leg_analys_tc(TsLegTab t, TsTcTab tc, const char *__restrict__ wimg, int w_nf
       }
     }
   };
-  ts_tc_persistent(smem, pp, S, stage, tmem, 256, sc, epilogue);
+  ts_tc_persistent(smem, pp, S, TS_TC_ASLOTS, stage, tmem, 128, 256u, sc, epilogue);
   ts_tc_fence_before();
   __syncthreads();
   if (pp->bad && tid == 0) atomicExch(tc.err, 1);

@@ -99,17 +99,18 @@ int kpar_h(int lmax, int m, int par) { return (lmax - m + 1 + 1 - par) / 2; }
 
 // Tile geometry of the tensor-core kernels, from the plan's sizes alone (so
 // the model compiler can size shared memory without the tables).  TS_TC_NL
-// (the synthesis latitude tile, a multiple of 16 <= 128) and TS_TC_LTL (the
-// analysis degree tile, a multiple of 16 <= 128: two 256-column accumulator
-// buffers) tune it, like the
-// reference's SHT_* knobs (src/sht/sht.ts:47-56).
+// (the synthesis latitude tile, a multiple of 16 <= 96: two accumulator
+// buffers of 2*NL columns and two 64-column operand slots fit in the 512
+// TMEM columns) and TS_TC_LTL (the analysis degree tile, a multiple of
+// 16 <= 128: two 128-column accumulator buffers and four operand slots) tune
+// it, like the reference's SHT_* knobs (src/sht/sht.ts:47-56).
 TsTcGeom ts_tc_geom(ts_plan p) {
   TsTcGeom g;
-  int nl_cap = 96;  // two accumulator buffers of 2*NL columns fit in 512
+  int nl_cap = 96;
   if (p->tune_nl > 0)
-    nl_cap = std::max(16, std::min(128, p->tune_nl & ~15));
+    nl_cap = std::max(16, std::min(96, p->tune_nl & ~15));
   else if (const char *e = getenv("TS_TC_NL"))
-    nl_cap = std::max(16, std::min(128, atoi(e) & ~15));
+    nl_cap = std::max(16, std::min(96, atoi(e) & ~15));
   g.NL = std::min(nl_cap, ((p->nh + 15) / 16) * 16);
   g.nLT = (p->nh + g.NL - 1) / g.NL;
   g.LTL = 128;
@@ -423,12 +424,13 @@ size_t ts_tc_bytes(ts_plan p) { return p->tc ? static_cast<ts_tc_tables *>(p->tc
 // pipeline depth and shared memory of the two persistent kernels
 namespace {
 const size_t kSmemBudget = 227 * 1024 - 2048;
-size_t synth_stage(ts_plan p) { return 2 * 16384 + 2 * (size_t)ts_tc_geom(p).NL * 128; }
+size_t synth_stage(ts_plan p) { return TS_TC_STAGE_A + 2 * (size_t)ts_tc_geom(p).NL * 128; }
 int synth_stages(ts_plan p) {
-  return (int)std::min<size_t>(TS_TC_MAXSTAGE, (kSmemBudget - 2 * TS_TC_SYN_STAGING) / synth_stage(p));
+  return (int)std::min<size_t>(TS_TC_MAXSTAGE,
+                               (kSmemBudget - 2 * TS_TC_SYN_NSTG * TS_TC_SYN_STAGING) / synth_stage(p));
 }
 int analys_N(ts_plan p) { return std::min(ts_tc_geom(p).LTL, ((kpar_h(p->lmax, 0, 0) + 15) / 16) * 16); }
-size_t analys_stage(ts_plan p) { return 2 * 16384 + 2 * (size_t)analys_N(p) * 128; }
+size_t analys_stage(ts_plan p) { return TS_TC_STAGE_A + 2 * (size_t)analys_N(p) * 128; }
 size_t analys_staging(ts_plan p) {
   return 2 * (size_t)std::min(analys_N(p), TS_TC_ANA_COLS) * 2 * TS_TC_ANA_ROW * 4;
 }
@@ -441,7 +443,8 @@ int ts_tc_analys_stages(ts_plan p) {
 int ts_tc_analys_nmax(ts_plan p) { return analys_N(p); }
 
 size_t ts_tc_synth_smem(ts_plan p) {
-  return synth_stages(p) * synth_stage(p) + 2 * TS_TC_SYN_STAGING + 1024 + sizeof(TsTcPipe);
+  return synth_stages(p) * synth_stage(p) + 2 * TS_TC_SYN_NSTG * TS_TC_SYN_STAGING + 1024 +
+         sizeof(TsTcPipe);
 }
 
 size_t ts_tc_analys_smem(ts_plan p) {
