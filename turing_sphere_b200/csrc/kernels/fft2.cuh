@@ -411,39 +411,54 @@ TS_DEV void ts_f2_forward_in(float2 *b, const float2 *twq, const float *__restri
 // s = X[k] + conj X[H-k] and u = i e^{2 pi i k/nphi} (X[k] - conj X[H-k]),
 // Z[k] = s + u and, as e^{2 pi i (H-k)/nphi} = -conj e^{2 pi i k/nphi},
 // Z[H-k] = conj(s - u).
-template <class C, class LatOf>
-TS_DEV void ts_f2_pack(float2 *b, const float2 *__restrict__ src, const TsFftTab &ft,
-                       LatOf lat_of) {
+// NS fields at once: field s from src + s * src_stride into the row block at
+// b + s * bs (the loads of every field are in flight together).
+template <class C, int NS, class LatOf>
+TS_DEV void ts_f2_pack_n(float2 *b, long bs, const float2 *__restrict__ src, long src_stride,
+                         const TsFftTab &ft, LatOf lat_of) {
   // thread t keeps row t % R and takes the pairs k = t / R + P j (T = P R)
   constexpr int H = C::H, NK = H / 2 + 1, NI = (NK + C::P - 1) / C::P;
   const int r = threadIdx.x % C::R, k0 = threadIdx.x / C::R;
   const int lat = lat_of(r);
-  const float2 *col = src + (lat >= 0 ? lat : 0);
-  float2 xk[NI], xh[NI];
+  float2 xk[NS][NI], xh[NS][NI];
 #pragma unroll
-  for (int j = 0; j < NI; j++) {
-    const int kk = k0 + C::P * j;
-    xk[j] = make_float2(0.f, 0.f);
-    xh[j] = make_float2(0.f, 0.f);
-    if (lat >= 0 && kk < NK) {
-      if (kk <= ft.mmax) xk[j] = col[(long)kk * ft.nlat];
-      if (H - kk <= ft.mmax) xh[j] = col[(long)(H - kk) * ft.nlat];
+  for (int s = 0; s < NS; s++) {
+    const float2 *col = src + s * src_stride + (lat >= 0 ? lat : 0);
+#pragma unroll
+    for (int j = 0; j < NI; j++) {
+      const int kk = k0 + C::P * j;
+      xk[s][j] = make_float2(0.f, 0.f);
+      xh[s][j] = make_float2(0.f, 0.f);
+      if (lat >= 0 && kk < NK) {
+        if (kk <= ft.mmax) xk[s][j] = col[(long)kk * ft.nlat];
+        if (H - kk <= ft.mmax) xh[s][j] = col[(long)(H - kk) * ft.nlat];
+      }
     }
   }
-  float2 *row = b + r * C::RP;
 #pragma unroll
   for (int j = 0; j < NI; j++) {
     const int kk = k0 + C::P * j;
     if (kk < NK) {
       const int h = H - kk;
-      const float2 x = kk == 0 ? make_float2(xk[j].x, 0.f) : xk[j];
-      const float2 ch = c_conj(xh[j]);
-      const float2 sp = c_add(x, ch);
-      const float2 u = c_mul_i(c_mul(c_sub(x, ch), __ldg(ft.tw + kk)));
-      row[kk] = c_add(sp, u);
-      if (kk > 0 && kk < h) row[h] = c_conj(c_sub(sp, u));
+      const float2 t = __ldg(ft.tw + kk);
+#pragma unroll
+      for (int s = 0; s < NS; s++) {
+        float2 *row = b + s * bs + r * C::RP;
+        const float2 x = kk == 0 ? make_float2(xk[s][j].x, 0.f) : xk[s][j];
+        const float2 ch = c_conj(xh[s][j]);
+        const float2 sp = c_add(x, ch);
+        const float2 u = c_mul_i(c_mul(c_sub(x, ch), t));
+        row[kk] = c_add(sp, u);
+        if (kk > 0 && kk < h) row[h] = c_conj(c_sub(sp, u));
+      }
     }
   }
+}
+
+template <class C, class LatOf>
+TS_DEV void ts_f2_pack(float2 *b, const float2 *__restrict__ src, const TsFftTab &ft,
+                       LatOf lat_of) {
+  ts_f2_pack_n<C, 1>(b, 0, src, 0, ft, lat_of);
 }
 
 // 2 X[k] of the analysis from the forward-transformed row and the twiddle
@@ -681,44 +696,139 @@ ts_f2_analys_w(TsFftTab ft, const float *__restrict__ spat, long spat_stride,
 //   gm [inst][NANA][mmax+1][nlat].
 // grid = (ceil(nlat/R) or ceil(nh/(R/2)), instances), block = P*R; shared
 // memory ts_f2_smem_bytes(max(NSYN, NANA, 1)).
-// phase 1 of the synthesis for the row block at b: Q-point DFTs over k2,
-// twiddles, transposed store (two barriers)
-template <class C>
-TS_DEV void ts_f2_inv_phase1(float2 *b, const float2 *twq) {
-  const int tid = threadIdx.x;
+
+// phase 1 of the synthesis for the row blocks at b + s bs (s < NS): Q-point
+// DFTs over k2, twiddles, transposed store (two barriers)
+template <class C, int NS>
+TS_DEV void ts_f2_inv_phase1_n(float2 *b, long bs, const float2 *twq) {
   int r, k1;
-  ts_f2_rk<C>(tid, r, k1);
-  float2 *row = b + r * C::RP;
-  float2 x[C::Q];
+  ts_f2_rk<C>(threadIdx.x, r, k1);
+  float2 x[NS][C::Q];
 #pragma unroll
-  for (int k2 = 0; k2 < C::Q; k2++) x[k2] = row[k1 + C::P * k2];
-  ts_dft<C::Q, +1>(x);
+  for (int s = 0; s < NS; s++) {
+    const float2 *row = b + s * bs + r * C::RP;
 #pragma unroll
-  for (int n2 = 1; n2 < C::Q; n2++) x[n2] = c_mul(x[n2], twq[n2 * C::P1 + k1]);
+    for (int k2 = 0; k2 < C::Q; k2++) x[s][k2] = row[k1 + C::P * k2];
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++) ts_dft<C::Q, +1>(x[s]);
+#pragma unroll
+  for (int n2 = 1; n2 < C::Q; n2++) {
+    const float2 t = twq[n2 * C::P1 + k1];
+#pragma unroll
+    for (int s = 0; s < NS; s++) x[s][n2] = c_mul(x[s][n2], t);
+  }
   __syncthreads();
 #pragma unroll
-  for (int n2 = 0; n2 < C::Q; n2++) row[n2 * C::P1 + k1] = x[n2];
+  for (int s = 0; s < NS; s++) {
+    float2 *row = b + s * bs + r * C::RP;
+#pragma unroll
+    for (int n2 = 0; n2 < C::Q; n2++) row[n2 * C::P1 + k1] = x[s][n2];
+  }
   __syncthreads();
 }
 
-// phase 2 of the analysis for the row block at b: Q-point DFTs over n2 from
-// the transposed layout, natural store (two barriers)
-template <class C>
-TS_DEV void ts_f2_fwd_phase2(float2 *b) {
-  const int tid = threadIdx.x;
+// phase 2 of the analysis for the row blocks at b + s bs (s < NS): Q-point
+// DFTs over n2 from the transposed layout, natural store (two barriers)
+template <class C, int NS>
+TS_DEV void ts_f2_fwd_phase2_n(float2 *b, long bs) {
   int r, k1;
-  ts_f2_rk<C>(tid, r, k1);
-  float2 *row = b + r * C::RP;
-  float2 x[C::Q];
+  ts_f2_rk<C>(threadIdx.x, r, k1);
+  float2 x[NS][C::Q];
 #pragma unroll
-  for (int n2 = 0; n2 < C::Q; n2++) x[n2] = row[n2 * C::P1 + k1];
-  ts_dft<C::Q, -1>(x);
+  for (int s = 0; s < NS; s++) {
+    const float2 *row = b + s * bs + r * C::RP;
+#pragma unroll
+    for (int n2 = 0; n2 < C::Q; n2++) x[s][n2] = row[n2 * C::P1 + k1];
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++) ts_dft<C::Q, -1>(x[s]);
   __syncthreads();
 #pragma unroll
-  for (int k2 = 0; k2 < C::Q; k2++) row[k1 + C::P * k2] = x[k2];
+  for (int s = 0; s < NS; s++) {
+    float2 *row = b + s * bs + r * C::RP;
+#pragma unroll
+    for (int k2 = 0; k2 < C::Q; k2++) row[k1 + C::P * k2] = x[s][k2];
+  }
   __syncthreads();
 }
 
+// ts_f2_write_w for NS fields f0 + s (row blocks b + s * bs): every value is
+// computed from shared memory first and the stores follow back to back, so
+// the reads of one k do not wait behind the stores of the previous one.  A
+// thread takes at most (Q + 1) / 2 orders (mmax < H).
+template <class C, int NS>
+TS_DEV void ts_f2_write_w_n(const float2 *b, long bs, int lat0, long f0, const TsFftTab &ft,
+                            const float *__restrict__ wq, char *wimg, int nfb, int fpb, int nlc,
+                            int nh, const int *__restrict__ w_kmin) {
+  constexpr int NPR = C::R / 2, KS = 2 * C::P, NIT = (C::Q + 1) / 2;
+  const int j = threadIdx.x % NPR;
+  const int lat = lat0 + j;
+  if (lat >= nh) return;
+  const bool south = ft.nlat - 1 - lat != lat;
+  const float w = 0.5f * __ldg(wq + lat);  // times 2 X[k] of both rows
+  // k groups as in ts_f2_write_w (the two halves of a half-warp 8 apart)
+  const int g = threadIdx.x / NPR;
+  const int k0 = KS % 16 == 0 ? (g & ~15) + ((g & 1) << 3) + ((g >> 1) & 7) : g;
+  const int kl0 = w_kmin ? __ldg(w_kmin + 2 * (lat >> 5)) : ft.mmax + 1;
+  const int kl1 = w_kmin ? __ldg(w_kmin + 2 * (lat >> 5) + 1) : ft.mmax + 1;
+  const int kend = min(ft.mmax + 1, max(kl0, kl1));
+  float2 t[NIT];
+#pragma unroll
+  for (int i = 0; i < NIT; i++)
+    t[i] = k0 + KS * i < kend ? __ldg(ft.tw + k0 + KS * i) : make_float2(0.f, 0.f);
+  float4 v[NS][NIT];  // w (N + S), w (N - S) of (re, im) per order
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+    const float2 *rn = b + s * bs + j * C::RP, *rs = b + s * bs + (NPR + j) * C::RP;
+#pragma unroll
+    for (int i = 0; i < NIT; i++) {
+      const int k = k0 + KS * i;
+      v[s][i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (k < kend) {
+        const float2 xn = ts_f2_xk2<C>(rn, k, t[i]);
+        const float2 xs = south ? ts_f2_xk2<C>(rs, k, t[i]) : make_float2(0.f, 0.f);
+        v[s][i] = make_float4(w * (xn.x + xs.x), w * (xn.y + xs.y), w * (xn.x - xs.x),
+                              w * (xn.y - xs.y));
+      }
+    }
+  }
+  const long kstep = (long)nfb * 2 * nlc * 16384, pstep = (long)nlc * 16384;
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+    const long f = f0 + s;
+    const long fb = f / fpb;
+    const int fl = (int)(f - fb * fpb);
+    const int o_re = ts_swz_img(2 * fl, lat & 31), o_im = ts_swz_img(2 * fl + 1, lat & 31);
+    char *base = wimg + ((long)fb * 2 * nlc + (lat >> 5)) * 16384;
+#pragma unroll
+    for (int i = 0; i < NIT; i++) {
+      const int k = k0 + KS * i;
+      char *blk = base + k * kstep;
+      if (k < kl0 && k < kend) {
+        *reinterpret_cast<float *>(blk + o_re) = v[s][i].x;
+        *reinterpret_cast<float *>(blk + o_im) = v[s][i].y;
+      }
+      if (k < kl1 && k < kend) {
+        *reinterpret_cast<float *>(blk + pstep + o_re) = v[s][i].z;
+        *reinterpret_cast<float *>(blk + pstep + o_im) = v[s][i].w;
+      }
+    }
+  }
+}
+
+// f(TsIC<s0>{}, TsIC<n>{}) for the groups [s0, s0 + n) of at most G of [0, N)
+template <int N, int G, int S0 = 0, class F>
+TS_DEV void ts_f2_groups(F &&f) {
+  if constexpr (S0 < N) {
+    f(TsIC<S0>{}, TsIC<(N - S0 < G ? N - S0 : G)>{});
+    ts_f2_groups<N, G, S0 + G>(f);
+  }
+}
+
+// Species go through the synthesis and analysis passes two at a time: one
+// pair of barriers and one batch of loads per pair (the registers of two
+// P-point rows per thread are what the middle section holds anyway).
 template <class Prog, int P, int Q, int R, bool PAIRED>
 __global__ void __launch_bounds__(P *R, TS_F2_PHASE_MINB(P, R))
 ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
@@ -734,12 +844,16 @@ ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
   const int lat0 = blockIdx.x * (PAIRED ? R / 2 : R);
   const TsF2Rows<C, PAIRED> rows{lat0, ft.nlat, io.nh};
   ts_f2_twq<C>(twq, ft);
-#pragma unroll 1
-  for (int s = 0; s < NSYN; s++)
-    ts_f2_pack<C>(buf + s * BS, io.fm + (inst * NSYN + s) * io.field, ft, rows);
+  ts_f2_groups<NSYN, 2>([&](auto s0c, auto nc) {
+    constexpr int s0 = decltype(s0c)::value, n = decltype(nc)::value;
+    ts_f2_pack_n<C, n>(buf + s0 * BS, BS, io.fm + (inst * NSYN + s0) * io.field, io.field, ft,
+                       rows);
+  });
   __syncthreads();
-#pragma unroll 1
-  for (int s = 0; s < NSYN; s++) ts_f2_inv_phase1<C>(buf + s * BS, twq);
+  ts_f2_groups<NSYN, 2>([&](auto s0c, auto nc) {
+    constexpr int s0 = decltype(s0c)::value, n = decltype(nc)::value;
+    ts_f2_inv_phase1_n<C, n>(buf + s0 * BS, BS, twq);
+  });
 
   // Thread (row r, n2) holds, after the synthesis's P-point DFTs, every
   // species at the grid points n = Q n1 + n2 (n1 < P): exactly the inputs
@@ -798,14 +912,19 @@ ts_f2_phase(TsFftTab ft, TsPhaseIO io) {
     }
   }
   __syncthreads();
+  ts_f2_groups<NANA, 2>([&](auto s0c, auto nc) {
+    constexpr int s0 = decltype(s0c)::value, n = decltype(nc)::value;
+    ts_f2_fwd_phase2_n<C, n>(buf + s0 * BS, BS);
+  });
+  if constexpr (PAIRED) {
+    ts_f2_groups<NANA, 2>([&](auto s0c, auto nc) {
+      constexpr int s0 = decltype(s0c)::value, n = decltype(nc)::value;
+      ts_f2_write_w_n<C, n>(buf + s0 * BS, BS, lat0, inst * NANA + s0, ft, io.wq, io.wimg,
+                            io.w_nfb, io.w_fpb, io.w_nlc, io.nh, io.w_kmin);
+    });
+  } else {
 #pragma unroll 1
-  for (int k = 0; k < NANA; k++) ts_f2_fwd_phase2<C>(buf + k * BS);
-#pragma unroll 1
-  for (int k = 0; k < NANA; k++) {
-    if constexpr (PAIRED)
-      ts_f2_write_w<C>(buf + k * BS, lat0, inst * NANA + k, ft, io.wq, io.wimg, io.w_nfb,
-                       io.w_fpb, io.w_nlc, io.nh, io.w_kmin);
-    else
+    for (int k = 0; k < NANA; k++)
       ts_f2_unpack<C>(buf + k * BS, io.gm + (inst * NANA + k) * io.field, ft, rows);
   }
 }
