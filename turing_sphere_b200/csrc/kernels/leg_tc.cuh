@@ -368,6 +368,24 @@ TS_DEV void ts_tc_split_tmem(const char *tile, unsigned taddr, int r) {
   }
 }
 
+// A position in a ring of n slots walked in order: the slot of the current
+// stage and the parity of that slot's current use (the uses of a slot
+// alternate parity, and every slot flips once per round).  Counters instead
+// of stage / n and stage % n keep integer division out of the roles' loops.
+struct TsRing {
+  int slot, n;
+  unsigned phase;  // parity of the current use
+  bool wrapped;    // past the first round: every slot has been used before
+  TS_DEV explicit TsRing(int n_) : slot(0), n(n_), phase(0), wrapped(false) {}
+  TS_DEV void next() {
+    if (++slot == n) {
+      slot = 0;
+      phase ^= 1u;
+      wrapped = true;
+    }
+  }
+};
+
 // MMA issue (one thread): per tile, wait until the epilogue has drained the
 // accumulator buffer, then per stage wait for the split data tile in TMEM
 // slot a (the split warps waited for the stage's copies, table included),
@@ -379,7 +397,8 @@ template <class Sched>
 TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, int NA, unsigned stage_bytes,
                            unsigned tmem, int acc_cols, unsigned a_col0, const Sched &sc) {
   const int ntiles = sc.ntiles();
-  long g = 0;
+  const unsigned smem0 = ts_smem_u32(smem) + TS_TC_STAGE_A;
+  TsRing rs(S), ra(NA);
   int i = 0;
   for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x, i++) {
     const int b = i & 1;
@@ -392,27 +411,31 @@ TS_DEV void ts_tc_mma_role(char *smem, TsTcPipe *pp, int S, int NA, unsigned sta
     const int T = sc.stages(ti);
     const unsigned tb = sc.table_bytes(ti);
     const unsigned idesc = ts_idesc_tf32(sc.n(ti));
-    for (int t_ = 0; t_ < T; t_++, g++) {
-      const int s = (int)(g % S), a = (int)(g % NA);
-      const unsigned ause = (unsigned)(g / NA);
-      if (!ts_mbar_wait(&pp->a_full[a], ause & 1, pp->limit)) {
+    const unsigned dbase = tmem + (unsigned)(b * acc_cols);
+    for (int t_ = 0; t_ < T; t_++, rs.next(), ra.next()) {
+      if (!ts_mbar_wait(&pp->a_full[ra.slot], ra.phase, pp->limit)) {
         ts_tc_flag(pp);
         return;
       }
       ts_tc_fence_after();
-      const unsigned bhi = ts_smem_u32(smem + s * stage_bytes) + TS_TC_STAGE_A, blo = bhi + tb / 2;
-      const unsigned ahi = tmem + a_col0 + 64u * (unsigned)a, alo = ahi + 32;
-      const unsigned d = tmem + (unsigned)(b * acc_cols + sc.d_col(ti, t_));
-      const bool init = sc.first(ti, t_);
+      // k-step kk reads the 32 bytes at kk * 32 of each 128-byte row: the
+      // descriptor's start-address field (address >> 4) advances by 2
+      const unsigned bhi = smem0 + (unsigned)rs.slot * stage_bytes;
+      const unsigned long long dhi = ts_umma_desc(bhi), dlo = ts_umma_desc(bhi + tb / 2);
+      const unsigned ahi = tmem + a_col0 + 64u * (unsigned)ra.slot, alo = ahi + 32;
+      int dcol;
+      bool init;
+      sc.stage_acc(ti, t_, dcol, init);
+      const unsigned d = dbase + (unsigned)dcol;
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) {
         const unsigned acc = (!init || kk > 0) ? 1u : 0u;
-        ts_mma_tf32_ta(d, ahi + kk * 8, ts_umma_desc(bhi + kk * 32), idesc, acc);
-        ts_mma_tf32_ta(d, ahi + kk * 8, ts_umma_desc(blo + kk * 32), idesc, 1u);
-        ts_mma_tf32_ta(d, alo + kk * 8, ts_umma_desc(bhi + kk * 32), idesc, 1u);
+        ts_mma_tf32_ta(d, ahi + kk * 8, dhi + 2 * kk, idesc, acc);
+        ts_mma_tf32_ta(d, ahi + kk * 8, dlo + 2 * kk, idesc, 1u);
+        ts_mma_tf32_ta(d, alo + kk * 8, dhi + 2 * kk, idesc, 1u);
       }
-      ts_mma_commit(&pp->empty[s]);
-      ts_mma_commit(&pp->a_empty[a]);
+      ts_mma_commit(&pp->empty[rs.slot]);
+      ts_mma_commit(&pp->a_empty[ra.slot]);
     }
     ts_mma_commit(&pp->acc_full[b]);
   }
@@ -435,45 +458,42 @@ TS_DEV void ts_tc_persistent(char *smem, TsTcPipe *pp, int S, int NA, unsigned s
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntiles = sc.ntiles();
   if (warp < 4) {
-    long g = 0;
+    TsRing rs(S), ra(NA);
     const unsigned lanebase = tmem + ((unsigned)(warp * 32) << 16) + a_col0;
     for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x) {
       const int T = sc.stages(tile);
-      for (int t_ = 0; t_ < T; t_++, g++) {
-        const int s = (int)(g % S), a = (int)(g % NA);
-        const unsigned use = (unsigned)(g / S), ause = (unsigned)(g / NA);
-        if (!ts_mbar_wait(&pp->full[s], use & 1, pp->limit) ||
-            (ause > 0 && !ts_mbar_wait(&pp->a_empty[a], (ause - 1) & 1, pp->limit))) {
+      for (int t_ = 0; t_ < T; t_++, rs.next(), ra.next()) {
+        if (!ts_mbar_wait(&pp->full[rs.slot], rs.phase, pp->limit) ||
+            (ra.wrapped && !ts_mbar_wait(&pp->a_empty[ra.slot], ra.phase ^ 1u, pp->limit))) {
           ts_tc_flag(pp);
           return;
         }
         ts_tc_fence_after();  // the stores follow the MMAs that read the slot before
-        ts_tc_split_tmem(smem + s * stage_bytes, lanebase + 64u * (unsigned)a, tid);
+        ts_tc_split_tmem(smem + rs.slot * stage_bytes, lanebase + 64u * (unsigned)ra.slot, tid);
         ts_tmem_wait_st();
         ts_tc_fence_before();
         __syncwarp();
-        if (lane == 0) ts_mbar_arrive(&pp->a_full[a]);
+        if (lane == 0) ts_mbar_arrive(&pp->a_full[ra.slot]);
       }
     }
   } else if (warp == 4) {
     if (lane == 0 && !sc.tc->stall_copies) {
-      long g = 0;
+      TsRing rs(S);
+      int g = 0;  // stages issued
       for (int tile = blockIdx.x; tile < ntiles && !ts_tc_bad(pp); tile += gridDim.x) {
         const auto ti = sc.tile(tile);
         const int T = sc.stages(ti);
         const unsigned tb = sc.table_bytes(ti);
         int t_ = 0;
-        for (; t_ < T; t_++, g++) {
-          const int s = (int)(g % S);
-          const unsigned use = (unsigned)(g / S);
-          if (use > 0 && !ts_mbar_wait(&pp->empty[s], (use - 1) & 1, pp->limit)) {
+        for (; t_ < T; t_++, g++, rs.next()) {
+          if (rs.wrapped && !ts_mbar_wait(&pp->empty[rs.slot], rs.phase ^ 1u, pp->limit)) {
             ts_tc_flag(pp);
             break;
           }
-          char *st = smem + s * stage_bytes;
-          ts_mbar_arrive_tx(&pp->full[s], TS_TC_STAGE_A + tb);
-          ts_bulk_g2s(st, sc.a_src(ti, t_), TS_TC_STAGE_A, &pp->full[s]);
-          ts_bulk_g2s(st + TS_TC_STAGE_A, sc.b_src(ti, t_), tb, &pp->full[s]);
+          char *st = smem + rs.slot * stage_bytes;
+          ts_mbar_arrive_tx(&pp->full[rs.slot], TS_TC_STAGE_A + tb);
+          ts_bulk_g2s(st, sc.a_src(ti, t_), TS_TC_STAGE_A, &pp->full[rs.slot]);
+          ts_bulk_g2s(st + TS_TC_STAGE_A, sc.b_src(ti, t_), tb, &pp->full[rs.slot]);
         }
         if (t_ < T) break;
       }
@@ -578,15 +598,13 @@ struct TsSynthSched {
     parcc(ti, t_, par, cc);
     return ti.b + (long)((par ? ti.n0 : 0) + cc) * nLT * 2 * NL * 128;
   }
-  TS_DEV int d_col(const Tile &ti, int t_) const {
+  // accumulator column of stage t_ (its parity's half) and whether it starts
+  // the accumulation
+  TS_DEV void stage_acc(const Tile &ti, int t_, int &dcol, bool &first) const {
     int par, cc;
     parcc(ti, t_, par, cc);
-    return par * NL;
-  }
-  TS_DEV bool first(const Tile &ti, int t_) const {
-    int par, cc;
-    parcc(ti, t_, par, cc);
-    return cc == ti.cs;
+    dcol = par * NL;
+    first = cc == ti.cs;
   }
 };
 
@@ -768,8 +786,10 @@ struct TsAnalysSched {
   TS_DEV unsigned table_bytes(const Tile &ti) const { return ti.tb; }
   TS_DEV const char *a_src(const Tile &ti, int c) const { return ti.w + (long)c * 16384; }
   TS_DEV const char *b_src(const Tile &ti, int c) const { return ti.b + (long)c * ti.tb; }
-  TS_DEV int d_col(const Tile &, int) const { return 0; }
-  TS_DEV bool first(const Tile &, int c) const { return c == 0; }
+  TS_DEV void stage_acc(const Tile &, int c, int &dcol, bool &first) const {
+    dcol = 0;
+    first = c == 0;
+  }
 };
 
 // grid = min(#SMs, tiles), block = 448, persistent.  Tiles with no l values
