@@ -62,6 +62,19 @@ TS_DEV void ts_mbar_init(unsigned long long *bar, unsigned count) {
 // after `limit` polls and returns false.
 TS_DEV bool ts_mbar_wait(unsigned long long *bar, unsigned parity, unsigned limit) {
   const unsigned addr = ts_smem_u32(bar);
+  {
+    // a phase that has already completed (the usual case on the MMA thread's
+    // path) is seen by the non-blocking test without the try_wait's latency
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
   for (unsigned i = 0; i < limit; i++) {
     unsigned done;
     asm volatile(
