@@ -17,11 +17,10 @@
 // byte layout (TsTcImg; written by a relayout kernel for the synthesis and by
 // the Fourier analysis itself for the analysis).  The split data operand then
 // lives in tensor memory: the MMAs read A (hi, lo) from TMEM and only B (the
-// table) from shared memory.  An MMA of 128 x N x 8 reading both operands from
-// shared memory needs (4 KB + N * 32 B) per 2 * 128 * N * 8 flops, more than
-// the shared-memory bandwidth at the TF32 rate for N = 96, with the copies,
-// the split and the epilogue staging competing for the same banks; with A in
-// TMEM a stage moves 40% fewer shared-memory bytes.  The kernels are persistent
+// table) from shared memory.  A stage then moves about 40% fewer
+// shared-memory bytes (no A reads by the MMAs, no hi/lo stores by the split),
+// and a ring slot needs 16 KB less, which buys a fourth slot and
+// double-buffered epilogue staging.  The kernels are persistent
 // (one CTA per SM walking tiles blockIdx.x + k*gridDim.x) with 448 threads in
 // fixed roles: warps 0-3 split each data tile row by row (thread = row = TMEM
 // lane) into rna-rounded TF32 hi and lo in an NA-slot TMEM operand ring, warp 4
